@@ -1,0 +1,219 @@
+/*
+ * tse_cuda.h -- C-ABI of libtsecuda.so, the sm_100a implementation of the
+ * TRANSPORTSE time-step core.
+ *
+ * The reference (thkempka/transportse, tse.py) has no foreign-function
+ * interface: its kernels are numba functions called from the Python driver
+ * loop.  Each entry point below replaces one of those functions, keeps its
+ * argument meaning and its return values, and is called from the Python
+ * driver (transportse_b200.driver) through ctypes.
+ *
+ * Conventions
+ *  - All array pointers are DEVICE pointers to C-order (nx, ny, nz) float64
+ *    arrays (k fastest), the layout of tse.py:81-157.  Species fields are
+ *    passed one species at a time as contiguous (nx, ny, nz) arrays.
+ *  - The caller owns every buffer.  Entry points that need scratch take a
+ *    caller-provided device workspace whose size is returned by
+ *    tse_workspace_bytes(); nothing allocates on the hot path.
+ *  - Every call is stream-ordered on the given stream (a cudaStream_t passed
+ *    as void*; NULL = legacy default stream) and returns before the work
+ *    completes.  Solver results go to a device-resident TseSolveStatus,
+ *    readable after the stream is synchronised.
+ *  - Return value: TSE_OK, or a negative TSE_ERR_* code for invalid
+ *    arguments, a too-small workspace or a failed launch.
+ *  - Bounded waits: the persistent solver kernels synchronise their blocks
+ *    with a grid barrier whose wait is bounded in time; on timeout they set
+ *    TseSolveStatus.error = TSE_STATUS_BARRIER_TIMEOUT and return.
+ *  - Re-entrant across streams when each stream has its own workspace and
+ *    status buffers.
+ */
+#ifndef TSE_CUDA_H
+#define TSE_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TSE_OK 0
+#define TSE_ERR_ARG (-1)
+#define TSE_ERR_WORKSPACE (-2)
+#define TSE_ERR_LAUNCH (-3)
+#define TSE_ERR_DEVICE (-4)
+
+#define TSE_STATUS_OK 0
+#define TSE_STATUS_BARRIER_TIMEOUT 1
+
+/* Grid geometry: the module-level globals dx, dy, dz, g and beta that the
+ * reference kernels read (tse.py:82-96).  sin_beta / cos_beta are
+ * numpy.sin(beta) / numpy.cos(beta) evaluated on the host. */
+typedef struct TseGrid {
+    int32_t nx, ny, nz, reserved;
+    const double *dx, *dy, *dz; /* device, lengths nx, ny, nz */
+    double g, sin_beta, cos_beta;
+} TseGrid;
+
+/* Result of one solver call: the tuple the reference functions return
+ * (t, dt, converged, num_it) plus diagnostics.  Up to 8 dt-halving events
+ * (iteration, dt before halving, L2 at that iteration) are recorded for the
+ * log lines of tse.py:730-732, 902-904, 1070-1071. */
+typedef struct TseSolveStatus {
+    double t;          /* t_P / t_C / t_T: accumulated dt of the solve */
+    double dt;         /* dt_P / dt_C / dt_T: next time-step size */
+    double diff;       /* last relative L2 change */
+    int32_t converged;
+    int32_t num_it;
+    int32_t num_sub_it;
+    int32_t halvings;
+    int32_t error;     /* TSE_STATUS_* */
+    int32_t n_events;
+    int32_t ev_it[8];
+    double ev_dt[8];
+    double ev_diff[8];
+} TseSolveStatus;
+
+/* Pressure solve arguments, compute_P(P, c_f, nue, rho_f, phi, Kx, Ky, Kz,
+ * qx, qy, qz, dt_P, BP, WP, SOR, max_it, inc_it, max_dt, min_dt, P_conv)
+ * (tse.py:647-650).  qx/qy/qz are not read by the reference solve and are
+ * omitted.  c_r is the compressibility array numba froze at first call. */
+typedef struct TsePressureArgs {
+    double *P;        /* in/out */
+    double *Pn;       /* out: P at entry (the returned Pn) */
+    const double *c_f, *nue, *rho_f, *phi, *Kx, *Ky, *Kz, *c_r, *BP, *WP;
+    double dt_P, SOR, inc_it, max_dt, min_dt, P_conv;
+    int32_t max_it, reserved;
+} TsePressureArgs;
+
+/* Species transport arguments, compute_C(C, D_fx, D_fy, D_fz, phi, rho_f,
+ * qx, qy, qz, dt_C, BC, WC, RC, e, omega, SOR, max_it, inc_it, max_dt,
+ * min_dt, C_conv) (tse.py:783-786); l_l / l_t are the frozen lf_l / lf_t
+ * and imblflo the frozen config.C_IMBLFLO. */
+typedef struct TseSpeciesArgs {
+    double *C;        /* in/out, one species */
+    const double *D_fx, *D_fy, *D_fz, *phi, *rho_f, *qx, *qy, *qz, *BC, *WC, *RC, *e;
+    const double *l_l, *l_t;
+    double dt, omega, SOR, inc_it, max_dt, min_dt, conv;
+    int32_t max_it, imblflo;
+} TseSpeciesArgs;
+
+/* Heat transport arguments, compute_T(T, l_f, cp_f, rho_f, phi, qx, qy, qz,
+ * dt_T, BT, WT, e, omega, SOR, max_it, inc_it, max_dt, min_dt, T_conv)
+ * (tse.py:919-922); l_r / rho_r / cp_r / l_l / l_t are the frozen l_r,
+ * rho_r, cp_r, lt_l, lt_t and imblflo the frozen config.T_IMBLFLO. */
+typedef struct TseHeatArgs {
+    double *T;        /* in/out, one temperature layer */
+    const double *l_f, *cp_f, *rho_f, *phi, *qx, *qy, *qz, *BT, *WT, *e;
+    const double *l_r, *rho_r, *cp_r, *l_l, *l_t;
+    double dt, omega, SOR, inc_it, max_dt, min_dt, conv;
+    int32_t max_it, imblflo;
+} TseHeatArgs;
+
+/* Workspace kinds for tse_workspace_bytes(). */
+#define TSE_WS_PRESSURE 1
+#define TSE_WS_TRANSPORT 2
+#define TSE_WS_REDUCE 3
+
+/* Bytes of device workspace a call of the given kind needs for this grid. */
+size_t tse_workspace_bytes(const TseGrid *grid, int32_t kind);
+
+/* Red-black SOR pressure solve with the convergence / dt-halving loop of
+ * compute_P (tse.py:647-742), FP64, reference operation order.  Replaces
+ * tse.py:647. */
+int32_t tse_compute_P(const TseGrid *grid, const TsePressureArgs *args,
+                      TseSolveStatus *d_status, void *d_workspace,
+                      size_t workspace_bytes, void *stream);
+
+/* Darcy face fluxes, compute_q (tse.py:744-780); the last plane of each
+ * component is left untouched as in the reference.  Replaces tse.py:744. */
+int32_t tse_compute_q(const TseGrid *grid, const double *P, const double *BP,
+                      const double *Kx, const double *Ky, const double *Kz,
+                      double *qx, double *qy, double *qz, const double *nue,
+                      const double *rho_f, void *stream);
+
+/* Local flow-balance error, flow_error (tse.py:409-446).  Replaces
+ * tse.py:409. */
+int32_t tse_flow_error(const TseGrid *grid, const double *P, const double *Pn,
+                       const double *qx, const double *qy, const double *qz,
+                       const double *WP, const double *phi, const double *c_f,
+                       const double *c_r, const double *rho_f, double dt_P,
+                       double *e, void *stream);
+
+/* Species transport solve, compute_C (tse.py:783-916).  Replaces
+ * tse.py:783. */
+int32_t tse_compute_C(const TseGrid *grid, const TseSpeciesArgs *args,
+                      TseSolveStatus *d_status, void *d_workspace,
+                      size_t workspace_bytes, void *stream);
+
+/* Heat transport solve, compute_T (tse.py:919-1081).  Replaces tse.py:919. */
+int32_t tse_compute_T(const TseGrid *grid, const TseHeatArgs *args,
+                      TseSolveStatus *d_status, void *d_workspace,
+                      size_t workspace_bytes, void *stream);
+
+/* Smolarkiewicz anti-diffusive velocities, smolarkiewicz (tse.py:1083-1116).
+ * Replaces tse.py:1083. */
+int32_t tse_smolarkiewicz(const TseGrid *grid, const double *C,
+                          const double *qx, const double *qy, const double *qz,
+                          double *vx, double *vy, double *vz, double dt,
+                          double eps, double Sc, void *stream);
+
+/* Relative L2 change, l2_norm (tse.py:273-281), NaN -> 1; result written to
+ * d_out[0].  Replaces tse.py:273. */
+int32_t tse_l2_norm(const double *New, const double *Old, int64_t n,
+                    double *d_out, void *d_workspace, size_t workspace_bytes,
+                    void *stream);
+
+/* CFL limit of the driver (tse.py:1241-1249), reshape semantics included;
+ * d_out[0] = dt_CFL.  Replaces tse.py:1241-1249. */
+int32_t tse_dt_cfl(const TseGrid *grid, const double *qx, const double *qy,
+                   const double *qz, const double *phi, double *d_out,
+                   void *d_workspace, size_t workspace_bytes, void *stream);
+
+/* Neumann limit explicit_C (tse.py:385-396) over nspec (<= 8) species
+ * arrays; h_D is a HOST array of nspec device pointers; d_out[0] = dt_NeC.
+ * Replaces tse.py:385. */
+int32_t tse_explicit_C(const TseGrid *grid, const double *const *h_D,
+                       int32_t nspec, const double *phi, double *d_out,
+                       void *d_workspace, size_t workspace_bytes, void *stream);
+
+/* Field statistics used by the driver (species skip test tse.py:1300-1301,
+ * printout tse.py:1280-1285): d_out = {sum, max, min} in FP64, NaN
+ * propagating for max/min like numpy. */
+int32_t tse_field_stats(const double *x, int64_t n, double *d_out,
+                        void *d_workspace, size_t workspace_bytes, void *stream);
+
+/* Declared linear equation of state, the GPU form of the per-cell callback
+ * run by run_fluid_properties (tse.py:179-199):
+ *   rho_f = rho0 + a[0]*C[s[0]] + ... + a[m-1]*C[s[m-1]] - tcoef*(T - T0)
+ * evaluated left to right (m <= 8 terms).  h_C is a HOST array of species
+ * device pointers indexed by h_sidx. */
+int32_t tse_eos_linear(const TseGrid *grid, const double *const *h_C,
+                       const int32_t *h_sidx, const double *h_coef, int32_t m,
+                       const double *T, double rho0, double tcoef, double T0,
+                       double *rho_f, void *stream);
+
+/* Peclet maxima peclet_C / peclet_T (tse.py:331-383), printed diagnostics:
+ * d_out[0..2] = max Pe_x, Pe_y, Pe_z over non-boundary cells (NaN
+ * propagating; cells on the boundary count as 0 as the zero-initialised
+ * arrays of the reference do).  h_Dx/h_Dy/h_Dz are HOST arrays of nspec
+ * (<= 8) device pointers. */
+int32_t tse_peclet_C(const TseGrid *grid, const double *qx, const double *qy,
+                     const double *qz, const double *const *h_Dx,
+                     const double *const *h_Dy, const double *const *h_Dz,
+                     int32_t nspec, const double *BC, double *d_out,
+                     void *d_workspace, size_t workspace_bytes, void *stream);
+int32_t tse_peclet_T(const TseGrid *grid, const double *qx, const double *qy,
+                     const double *qz, const double *rho_f, const double *cp_f,
+                     const double *phi, const double *l_r, const double *l_f,
+                     const double *BT, double *d_out, void *d_workspace,
+                     size_t workspace_bytes, void *stream);
+
+/* Library version string. */
+const char *tse_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TSE_CUDA_H */

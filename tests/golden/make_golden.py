@@ -1,0 +1,170 @@
+"""Generate the golden fixtures in this folder by running the reference.
+
+The reference (thkempka/transportse) is one Python/numba script, ``tse.py``.
+This script executes it UNMODIFIED, from a read-only checkout, inside a fresh
+namespace (``exec``), once per synthetic config:
+
+* unit fixtures (``unit_*.npz``): the reference's numba kernels
+  (``compute_P``, ``compute_q``, ``flow_error``, ``compute_C``, ``compute_T``,
+  ``smolarkiewicz``, ``explicit_C``, ``l2_norm``) are called directly on seeded
+  random inputs and their outputs are stored beside the inputs.  Running the
+  script with ``t = 0`` defines every kernel without stepping (its final
+  summary then divides by zero steps, which is caught).
+* end-to-end fixtures (``e2e_*.npz``): a step-counting ``dynamic_bc`` callback
+  (tse.py:1448-1458; it returns every field unchanged) records the state after
+  each time step and stops the run after N steps.
+
+Usage:  python tests/golden/make_golden.py [--reference PATH] [--only NAME]
+
+It needs the reference checkout and numba, so it runs on the development
+machine only; the fixtures it writes are committed.
+"""
+from __future__ import annotations
+
+import argparse
+import contextlib
+import io
+import os
+import sys
+import uuid
+
+import numpy
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from transportse_b200 import workloads  # noqa: E402
+from tests.golden import cases  # noqa: E402
+
+
+class StopRun(Exception):
+    pass
+
+
+def _exec_reference(ref, cfg, taps=None):
+    """exec tse.py with ``cfg`` as its config module; return the namespace."""
+    import numba  # noqa: F401  (the reference needs it)
+    name = "tsecfg_" + uuid.uuid4().hex[:10]
+    cfg.__name__ = name
+    if getattr(cfg, "JITFLUPRO", False):
+        cfg.fluid_properties = numba.njit(cfg.fluid_properties)
+    sys.modules[name] = cfg
+    ns = {"__name__": "__tse_reference__"}
+    cfg._ns = ns
+    argv = sys.argv
+    sys.argv = ["tse.py", name + ".py"]
+    src = open(os.path.join(ref, "tse.py")).read()
+    out = io.StringIO()
+    try:
+        with contextlib.redirect_stdout(out):
+            try:
+                exec(compile(src, os.path.join(ref, "tse.py"), "exec"), ns)
+            except StopRun:
+                pass
+            except ZeroDivisionError:
+                if ns.get("n_tsteps", 1) != 0:
+                    raise
+    finally:
+        sys.argv = argv
+        sys.modules.pop(name, None)
+    ns["__stdout__"] = out.getvalue()
+    return ns
+
+
+def reference_namespace(ref, cfg):
+    """Namespace with every kernel of tse.py defined and nothing stepped."""
+    cfg.t = 0.0
+    cfg.DYNAMICBC = False
+    return _exec_reference(ref, cfg)
+
+
+def run_reference(ref, cfg, steps, keep_steps, fields):
+    """Run ``steps`` time steps; record scalars every step, fields at keep_steps."""
+    rec = {"dt": [], "t_sim": [], "numitP": [], "numitC": [], "numitT": [],
+           "num_CFL": [], "dt_P": [], "dt_C": [], "dt_T": []}
+    snaps = {}
+    cfg.DYNAMICBC = True
+
+    def dynamic_bc(t, bc_inc, P, T, C, BP, BT, BC, WP, WT, WC, Kx, Ky, Kz, rho_f,
+                   nue, c_f, cp_f, qx, phi, l_f, l_r):
+        ns = cfg._ns
+        for k in rec:
+            rec[k].append(float(ns.get(k, numpy.nan)))
+        step = len(rec["dt"])
+        if step in keep_steps:
+            for f in fields:
+                snaps["%s@%d" % (f, step)] = numpy.array(ns[f], copy=True)
+        if step >= steps:
+            raise StopRun()
+        return bc_inc, P, T, C, BP, BT, BC, WP, WT, WC, Kx, Ky, Kz
+
+    cfg.dynamic_bc = dynamic_bc
+    ns = _exec_reference(ref, cfg)
+    out = {("s_" + k): numpy.array(v) for k, v in rec.items()}
+    out.update(snaps)
+    out["keep_steps"] = numpy.array(sorted(keep_steps))
+    out["steps"] = numpy.array(steps)
+    return out, ns
+
+
+def gen_unit(ref, variant):
+    cfg, inputs = cases.unit_inputs_with_cfg(variant)
+    ns = reference_namespace(ref, cfg)
+    res = cases.run_unit_calls(ns, inputs, variant)
+    data = {("in_" + k): v for k, v in inputs.items()}
+    data.update({("out_" + k): v for k, v in res.items()})
+    # values the reference kernels see for sin/cos of the slope (numba libm)
+    import numba
+
+    @numba.njit
+    def _sc(b):
+        return numpy.sin(b), numpy.cos(b)
+    s, c = _sc(numpy.radians(cfg.beta))
+    data["sin_beta"] = numpy.array(s)
+    data["cos_beta"] = numpy.array(c)
+    return data
+
+
+E2E = {
+    # name: (builder, kwargs, steps, keep_steps, fields)
+    "slice_2d": (workloads.slice_2d, {}, 200, {1, 2, 5, 10, 50, 100, 200},
+                 ("P", "C", "qx", "qz")),
+    "reservoir_3d": (workloads.reservoir_3d, {"nx": 12, "ny": 10, "nz": 8, "seed": 11},
+                     8, {1, 2, 4, 8}, ("P", "C", "T", "qx", "qy", "qz", "rho_f")),
+    "sloped_3d": (workloads.sloped_3d, {"nx": 10, "ny": 8, "nz": 6, "seed": 5},
+                  5, {1, 3, 5}, ("P", "C", "T", "qx", "qy", "qz")),
+    "ensemble_member": (workloads.ensemble_member, {"seed": 3, "shape": (9, 7, 8)},
+                        6, {1, 3, 6}, ("P", "C", "T", "qx", "qy", "qz")),
+    "serving_request": (workloads.serving_request, {"seed": 4, "n": 9},
+                        5, {1, 5}, ("P", "C", "T", "qz")),
+}
+
+
+def gen_e2e(ref, name):
+    builder, kw, steps, keep, fields = E2E[name]
+    cfg = builder(**kw)
+    data, ns = run_reference(ref, cfg, steps, keep, fields)
+    data["config_checksum"] = numpy.array(cases.config_checksum(builder(**kw)))
+    return data
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference", default=os.environ.get("TSE_REFERENCE", "/root/reference"))
+    ap.add_argument("--only", default=None)
+    a = ap.parse_args()
+    jobs = [("unit_a", lambda: gen_unit(a.reference, "a")),
+            ("unit_b", lambda: gen_unit(a.reference, "b"))]
+    jobs += [("e2e_" + n, (lambda n=n: gen_e2e(a.reference, n))) for n in E2E]
+    for name, fn in jobs:
+        if a.only and a.only != name:
+            continue
+        data = fn()
+        path = os.path.join(HERE, name + ".npz")
+        numpy.savez_compressed(path, **data)
+        print("wrote", path, "%.1f KB" % (os.path.getsize(path) / 1024))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,77 @@
+"""Test helpers: NumPy adaptor over the CUDA kernels, fixture loading, errors."""
+import os
+
+import numpy
+
+from tests.conftest import GOLDEN
+
+
+def load(name):
+    return numpy.load(os.path.join(GOLDEN, name + ".npz"))
+
+
+def unit_inputs(fixture):
+    return {k[3:]: fixture[k] for k in fixture.files if k.startswith("in_")}
+
+
+def rel_err(got, ref):
+    """max |got - ref| / max(|ref|max, tiny): relative to the field's scale."""
+    got = numpy.asarray(got, dtype=numpy.float64)
+    ref = numpy.asarray(ref, dtype=numpy.float64)
+    if got.shape != ref.shape:
+        raise AssertionError("shape %s != %s" % (got.shape, ref.shape))
+    nan_g, nan_r = numpy.isnan(got), numpy.isnan(ref)
+    if not numpy.array_equal(nan_g, nan_r):
+        return numpy.inf
+    g, r = got[~nan_r], ref[~nan_r]
+    if g.size == 0:
+        return 0.0
+    scale = max(numpy.max(numpy.abs(r)), 1e-300)
+    return float(numpy.max(numpy.abs(g - r)) / scale)
+
+
+class NumpyKernels:
+    """Reference kernel names over transportse_b200.kernels.Model, taking and
+    returning NumPy arrays (so tests/golden/cases.run_unit_calls can drive it)."""
+
+    def __init__(self, model):
+        self.m = model
+
+    def _np(self, x):
+        import torch
+        return x.detach().cpu().numpy().copy() if isinstance(x, torch.Tensor) else x
+
+    def compute_P(self, *a, **k):
+        r = self.m.compute_P(*a, **k)
+        return r[0], r[1], self._np(r[2]), self._np(r[3]), r[4], r[5]
+
+    def compute_q(self, *a, **k):
+        return tuple(self._np(x) for x in self.m.compute_q(*a, **k))
+
+    def flow_error(self, *a, **k):
+        return self._np(self.m.flow_error(*a, **k))
+
+    def compute_C(self, *a, **k):
+        r = self.m.compute_C(*a, **k)
+        return r[0], r[1], self._np(r[2]), r[3], r[4]
+
+    def compute_T(self, *a, **k):
+        r = self.m.compute_T(*a, **k)
+        return r[0], r[1], self._np(r[2]), r[3], r[4]
+
+    def smolarkiewicz(self, *a, **k):
+        return tuple(self._np(x) for x in self.m.smolarkiewicz(*a, **k))
+
+    def explicit_C(self, *a, **k):
+        return self.m.explicit_C(*a, **k)
+
+    def l2_norm(self, *a, **k):
+        return self.m.l2_norm(*a, **k)
+
+
+def model_for(cfg, device):
+    from transportse_b200.kernels import Model
+    m = Model.from_config(cfg, device=device)
+    m.freeze(cfg.c_r, cfg.l_r, cfg.rho_r, cfg.cp_r, cfg.lf_l, cfg.lf_t, cfg.lt_l, cfg.lt_t,
+             cfg.C_IMBLFLO, cfg.T_IMBLFLO)
+    return m

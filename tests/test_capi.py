@@ -1,0 +1,76 @@
+"""The C-ABI library builds for sm_100a, loads, and exports every entry point
+include/tse_cuda.h declares; the ctypes structs match the C structs field by
+field.  No compute calls (these run without a GPU)."""
+import ctypes as ct
+import os
+import re
+import subprocess
+
+import pytest
+
+from tests.conftest import ROOT
+from transportse_b200 import _native as N
+from transportse_b200 import build
+
+HEADER = os.path.join(ROOT, "include", "tse_cuda.h")
+
+
+def declared_symbols():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(tse_[a-zA-Z0-9_]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_symbol():
+    path = build.build()
+    lib = ct.CDLL(path)
+    syms = declared_symbols()
+    assert len(syms) >= 15
+    for s in syms:
+        assert hasattr(lib, s), s
+        assert s in N.SIGNATURES, "ctypes signature missing for " + s
+
+
+def test_version_string_without_gpu():
+    assert b"sm_100a" in N.lib().tse_version()
+
+
+def test_workspace_sizes_without_gpu():
+    g = N.TseGrid(60, 1, 30, 0, None, None, None, 9.81, 0.0, 1.0)
+    for kind in (N.TSE_WS_PRESSURE, N.TSE_WS_TRANSPORT, N.TSE_WS_REDUCE):
+        assert N.lib().tse_workspace_bytes(ct.byref(g), kind) > 0
+    g.nx = 0
+    assert N.lib().tse_workspace_bytes(ct.byref(g), N.TSE_WS_PRESSURE) == 0
+
+
+STRUCTS = {
+    "TseGrid": N.TseGrid, "TseSolveStatus": N.TseSolveStatus,
+    "TsePressureArgs": N.TsePressureArgs, "TseSpeciesArgs": N.TseSpeciesArgs,
+    "TseHeatArgs": N.TseHeatArgs,
+}
+
+
+def test_struct_layout_matches_header(tmp_path):
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "%s"' % HEADER,
+             "int main(void) {"]
+    for sname, cls in STRUCTS.items():
+        lines.append('printf("%s %%zu\\n", sizeof(%s));' % (sname, sname))
+        for fname, _ in cls._fields_:
+            lines.append('printf("%s.%s %%zu\\n", offsetof(%s, %s));' % (sname, fname, sname, fname))
+    lines.append("return 0; }")
+    c = tmp_path / "layout.c"
+    c.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.check_call(["gcc", str(c), "-o", str(exe)])
+    out = dict(l.rsplit(" ", 1) for l in subprocess.check_output([str(exe)]).decode().split("\n") if l)
+    for sname, cls in STRUCTS.items():
+        assert int(out[sname]) == ct.sizeof(cls), sname
+        for fname, _ in cls._fields_:
+            assert int(out["%s.%s" % (sname, fname)]) == getattr(cls, fname).offset, (sname, fname)
+
+
+def test_ops_fail_loudly_without_library(monkeypatch):
+    monkeypatch.setattr(N, "_lib", None)
+    monkeypatch.setattr(N, "LIB_PATH", "/nonexistent/libtsecuda.so")
+    with pytest.raises(RuntimeError):
+        N.lib()

@@ -1,0 +1,249 @@
+// FP64 red-black SOR pressure solve, compute_P (tse.py:647-742).
+//
+// The reference recomputes six transmissibilities (alpha, tse.py:249-260)
+// and four buoyancy terms (beta_g, tse.py:263-271) for every cell in every
+// sweep.  They do not change during a solve, so one assembly pass computes
+// them once, with the reference's operation order, and stores them per
+// colour in the compact colour-split layout; the persistent loop then
+// streams 11-13 coefficient words per cell-update and evaluates the update
+//   P = (1-SOR) P + SOR (Anew + A B + Cnew - C D + Enew + Gnew + Inew + I J
+//                        + Knew - K L + R Pn + WP) / (R + M)       (tse.py:691-695)
+// term by term in the same order, so each cell-update is bit-identical to the
+// reference's.  Compiled with --fmad=false.
+#include "tse_rbsolve.cuh"
+
+namespace tse {
+
+enum PArr {
+    PA_A = 0, PA_C, PA_E, PA_G, PA_I, PA_K,   // transmissibilities x+ x- y+ y- z+ z-
+    PA_AB, PA_CD, PA_IJ, PA_KL,               // buoyancy products
+    PA_RPN, PA_WP, PA_DEN,                    // R*Pn, WP, R+M
+    PA_S, PA_M, PA_PN,                        // storage numerator, M, Pn (reset)
+    PA_P,                                     // solution
+    PA_COUNT
+};
+
+struct PressureForm {
+    double* arr[2];   // per colour: PA_COUNT arrays of Ncal doubles
+    long long Ncal, SX;
+    int H;
+    int xgrav, zgrav;
+    double SOR;
+
+    __device__ __forceinline__ const double* a(int col, int k) const { return arr[col] + (long long)k * Ncal; }
+
+    __device__ __forceinline__ double update(int col, long long m, uint8_t f, double xold,
+                                             const double* Xo) const {
+        const double* b = arr[col];
+        double s = (f & F_XP) ? b[PA_A * Ncal + m] * __ldcg(Xo + m + SX) : 0.0;
+        s = s + (xgrav ? b[PA_AB * Ncal + m] : 0.0);
+        s = s + ((f & F_XM) ? b[PA_C * Ncal + m] * __ldcg(Xo + m - SX) : 0.0);
+        s = s - (xgrav ? b[PA_CD * Ncal + m] : 0.0);
+        s = s + ((f & F_YP) ? b[PA_E * Ncal + m] * __ldcg(Xo + m + H) : 0.0);
+        s = s + ((f & F_YM) ? b[PA_G * Ncal + m] * __ldcg(Xo + m - H) : 0.0);
+        const long long zo = (long long)(f >> 7);
+        s = s + ((f & F_ZP) ? b[PA_I * Ncal + m] * __ldcg(Xo + m + zo) : 0.0);
+        s = s + (zgrav ? b[PA_IJ * Ncal + m] : 0.0);
+        s = s + ((f & F_ZM) ? b[PA_K * Ncal + m] * __ldcg(Xo + m - 1 + zo) : 0.0);
+        s = s - (zgrav ? b[PA_KL * Ncal + m] : 0.0);
+        s = s + b[PA_RPN * Ncal + m];
+        s = s + b[PA_WP * Ncal + m];
+        return (1.0 - SOR) * xold + (SOR * s) / b[PA_DEN * Ncal + m];
+    }
+
+    // dt halving: P = Pn (tse.py:738) and the dt-dependent R terms
+    __device__ __forceinline__ void reassemble(int col, long long m, double dt) const {
+        double* b = arr[col];
+        const double pn = b[PA_PN * Ncal + m];
+        const double R = b[PA_S * Ncal + m] / dt;
+        b[PA_RPN * Ncal + m] = R * pn;
+        b[PA_DEN * Ncal + m] = R + b[PA_M * Ncal + m];
+        b[PA_P * Ncal + m] = pn;
+    }
+};
+
+// alpha (tse.py:249-260) for the face between cells o (first) and c
+__device__ __forceinline__ double alpha_(double K1, double K2, double n1, double n2, double r1,
+                                         double r2, double d1, double d2, double dden1,
+                                         double dden2) {
+    return harm2(K1, K2, d1, d2) / harm2(n1, n2, d1, d2) / (dden2 * (dden1 + dden2) * 0.5) *
+           harm2(r1, r2, d1, d2);
+}
+
+__global__ void assemble_p_kernel(TseGrid g, TsePressureArgs a, PressureForm F, uint8_t* mask0,
+                                  uint8_t* mask1, Layout L) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long total = (long long)L.nx * L.ny * L.nzp;
+    if (t >= total) return;
+    const int nx = L.nx, ny = L.ny, nz = L.nz;
+    const int k = (int)(t % L.nzp);
+    const long long row = t / L.nzp;
+    const int j = (int)(row % ny);
+    const int i = (int)(row / ny);
+    const long long m = t >> 1;
+    const int col = (i + j + k) & 1;
+    double* b = F.arr[col];
+    const long long N = F.Ncal;
+    uint8_t* msk = col ? mask1 : mask0;
+    if (k >= nz) {
+        for (int q = 0; q < PA_COUNT; ++q) b[q * N + m] = 0.0;
+        msk[m] = 0;
+        return;
+    }
+    const long long c = row * nz + k;
+    const long long sx = (long long)ny * nz;
+    const double *dx = g.dx, *dy = g.dy, *dz = g.dz;
+    const double *Kx = a.Kx, *Ky = a.Ky, *Kz = a.Kz, *nue = a.nue, *rho = a.rho_f;
+    double A_ = 0, B_ = 0, C_ = 0, D_ = 0, E_ = 0, G_ = 0, I_ = 0, J_ = 0, K_ = 0, L_ = 0;
+    if (i != nx - 1) {
+        const long long o = c + sx;
+        A_ = alpha_(Kx[o], Kx[c], nue[o], nue[c], rho[o], rho[c], dx[i + 1], dx[i], dx[i + 1], dx[i]);
+        B_ = amean2(rho[o], rho[c], dx[i + 1], dx[i]) * g.g * 0.5 * (dx[i + 1] + dx[i]) * g.sin_beta;
+    }
+    if (i != 0) {
+        const long long o = c - sx;
+        C_ = alpha_(Kx[c], Kx[o], nue[c], nue[o], rho[c], rho[o], dx[i], dx[i - 1], dx[i - 1], dx[i]);
+        D_ = amean2(rho[c], rho[o], dx[i], dx[i - 1]) * g.g * 0.5 * (dx[i] + dx[i - 1]) * g.sin_beta;
+    }
+    if (j != ny - 1) {
+        const long long o = c + nz;
+        E_ = alpha_(Ky[o], Ky[c], nue[o], nue[c], rho[o], rho[c], dy[j + 1], dy[j], dy[j + 1], dy[j]);
+    }
+    if (j != 0) {
+        const long long o = c - nz;
+        G_ = alpha_(Ky[c], Ky[o], nue[c], nue[o], rho[c], rho[o], dy[j], dy[j - 1], dy[j - 1], dy[j]);
+    }
+    if (k != nz - 1) {
+        const long long o = c + 1;
+        I_ = alpha_(Kz[o], Kz[c], nue[o], nue[c], rho[o], rho[c], dz[k + 1], dz[k], dz[k + 1], dz[k]);
+        J_ = amean2(rho[o], rho[c], dz[k + 1], dz[k]) * g.g * 0.5 * (dz[k + 1] + dz[k]) * g.cos_beta;
+    }
+    if (k != 0) {
+        const long long o = c - 1;
+        K_ = alpha_(Kz[c], Kz[o], nue[c], nue[o], rho[c], rho[o], dz[k], dz[k - 1], dz[k - 1], dz[k]);
+        L_ = amean2(rho[c], rho[o], dz[k], dz[k - 1]) * g.g * 0.5 * (dz[k] + dz[k - 1]) * g.cos_beta;
+    }
+    const double por = a.phi[c];
+    const double S = rho[c] * ((1 - por) * a.c_r[c] + por * a.c_f[c]);
+    const double R = S / a.dt_P;
+    const double M = A_ + C_ + E_ + G_ + I_ + K_;
+    const double pn = a.P[c];
+    a.Pn[c] = pn;
+    b[PA_A * N + m] = A_;
+    b[PA_C * N + m] = C_;
+    b[PA_E * N + m] = E_;
+    b[PA_G * N + m] = G_;
+    b[PA_I * N + m] = I_;
+    b[PA_K * N + m] = K_;
+    b[PA_AB * N + m] = A_ * B_;
+    b[PA_CD * N + m] = C_ * D_;
+    b[PA_IJ * N + m] = I_ * J_;
+    b[PA_KL * N + m] = K_ * L_;
+    b[PA_RPN * N + m] = R * pn;
+    b[PA_WP * N + m] = a.WP[c];
+    b[PA_DEN * N + m] = R + M;
+    b[PA_S * N + m] = S;
+    b[PA_M * N + m] = M;
+    b[PA_PN * N + m] = pn;
+    b[PA_P * N + m] = pn;
+    uint8_t f = neighbour_flags(i, j, k, nx, ny, nz);
+    if (!(a.BP[c] != 0.0)) f |= F_ACTIVE;
+    msk[m] = f;
+}
+
+// compact colour arrays -> natural (nx, ny, nz) layout
+__global__ void unpack_kernel(double* out, const double* X0, const double* X1, Layout L) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long total = (long long)L.nx * L.ny * L.nz;
+    if (t >= total) return;
+    const int k = (int)(t % L.nz);
+    const long long row = t / L.nz;
+    const int j = (int)(row % L.ny);
+    const int i = (int)(row / L.ny);
+    const long long m = (row * L.nzp + k) >> 1;
+    out[t] = ((i + j + k) & 1) ? X1[m] : X0[m];
+}
+
+size_t pressure_ws_bytes(const Layout& L, long long* Ncal_out) {
+    long long Ncal = (L.Nc + 31) & ~31LL;
+    if (Ncal_out) *Ncal_out = Ncal;
+    size_t b = 0;
+    b += align256(sizeof(GridBarrier));
+    b += align256((size_t)2 * kMaxBlocks * sizeof(double));
+    b += 2 * align256((size_t)Ncal);                               // masks
+    b += 2 * (size_t)PA_COUNT * Ncal * sizeof(double);            // arrays
+    return b;
+}
+
+}  // namespace tse
+
+using namespace tse;
+
+extern "C" int32_t tse_compute_P(const TseGrid* grid, const TsePressureArgs* args,
+                                 TseSolveStatus* d_status, void* d_ws, size_t ws_bytes,
+                                 void* stream_) {
+    if (!grid || !args || !d_status || !d_ws) return TSE_ERR_ARG;
+    if (grid->nx < 1 || grid->ny < 1 || grid->nz < 1) return TSE_ERR_ARG;
+    if (!args->P || !args->Pn || !args->c_f || !args->nue || !args->rho_f || !args->phi ||
+        !args->Kx || !args->Ky || !args->Kz || !args->c_r || !args->BP || !args->WP)
+        return TSE_ERR_ARG;
+    if (args->max_it < 1) return TSE_ERR_ARG;
+    cudaStream_t stream = (cudaStream_t)stream_;
+    Layout L = make_layout(grid->nx, grid->ny, grid->nz);
+    long long Ncal = 0;
+    if (pressure_ws_bytes(L, &Ncal) > ws_bytes) return TSE_ERR_WORKSPACE;
+    char* p = (char*)d_ws;
+    GridBarrier* bar = (GridBarrier*)p;
+    p += align256(sizeof(GridBarrier));
+    double* partials = (double*)p;
+    p += align256((size_t)2 * kMaxBlocks * sizeof(double));
+    uint8_t* mask0 = (uint8_t*)p;
+    p += align256((size_t)Ncal);
+    uint8_t* mask1 = (uint8_t*)p;
+    p += align256((size_t)Ncal);
+    double* arr0 = (double*)p;
+    double* arr1 = arr0 + (size_t)PA_COUNT * Ncal;
+
+    PressureForm F;
+    F.arr[0] = arr0;
+    F.arr[1] = arr1;
+    F.Ncal = Ncal;
+    F.SX = L.SX;
+    F.H = L.H;
+    F.xgrav = grid->sin_beta != 0.0;
+    F.zgrav = grid->cos_beta != 0.0;
+    F.SOR = args->SOR;
+
+    if (cudaMemsetAsync(bar, 0, sizeof(GridBarrier), stream) != cudaSuccess) return TSE_ERR_LAUNCH;
+    const long long total = (long long)L.nx * L.ny * L.nzp;
+    assemble_p_kernel<<<(unsigned)((total + kBlock - 1) / kBlock), kBlock, 0, stream>>>(
+        *grid, *args, F, mask0, mask1, L);
+    if (cudaGetLastError() != cudaSuccess) return TSE_ERR_LAUNCH;
+
+    SolveCtl ctl;
+    ctl.L = L;
+    ctl.Ncal = Ncal;
+    ctl.dt = args->dt_P;
+    ctl.inc_it = args->inc_it;
+    ctl.max_dt = args->max_dt;
+    ctl.min_dt = args->min_dt;
+    ctl.conv = args->P_conv;
+    ctl.max_it = args->max_it;
+    ctl.pressure_schedule = 1;
+    ctl.stop_on_first = 0;
+    ctl.X[0] = arr0 + (size_t)PA_P * Ncal;
+    ctl.X[1] = arr1 + (size_t)PA_P * Ncal;
+    ctl.mask[0] = mask0;
+    ctl.mask[1] = mask1;
+    ctl.partials = partials;
+    ctl.bar = bar;
+    ctl.status = d_status;
+    int rc = launch_rb_solve(F, ctl, stream);
+    if (rc != TSE_OK) return rc;
+
+    const long long nat = (long long)L.nx * L.ny * L.nz;
+    unpack_kernel<<<(unsigned)((nat + kBlock - 1) / kBlock), kBlock, 0, stream>>>(
+        args->P, ctl.X[0], ctl.X[1], L);
+    if (cudaGetLastError() != cudaSuccess) return TSE_ERR_LAUNCH;
+    return TSE_OK;
+}
