@@ -125,6 +125,24 @@ int32_t tse_compute_P(const TseGrid *grid, const TsePressureArgs *args,
                       TseSolveStatus *d_status, void *d_workspace,
                       size_t workspace_bytes, void *stream);
 
+/* Pressure solve that allocates nothing and takes no workspace.  It has no
+ * counterpart in the reference; it exists for callers that cannot allocate
+ * device memory themselves -- a host program whose device memory belongs to
+ * someone else's allocator and that can pass only its field buffers, or one
+ * whose time loop must not stall on cudaMalloc, which can synchronise the
+ * device.  Same arguments and results as tse_compute_P, except that the
+ * scratch is a fixed TSE_NOALLOC_SCRATCH_BYTES (6 MiB) device array inside
+ * the library, reserved on every GPU that loads it until the process exits.
+ * That holds grids of up to about 43,000 cells (32 x 32 x 32 fits); larger
+ * grids return TSE_ERR_WORKSPACE and launch nothing.  The first call on a
+ * device looks up the array's device address, so make that first call before
+ * any stream capture.  All calls on one GPU share the array: calls that
+ * overlap on the GPU (other streams or host threads) race and must be
+ * serialised by the caller. */
+#define TSE_NOALLOC_SCRATCH_BYTES (6 * 1024 * 1024)
+int32_t tse_compute_P_noalloc(const TseGrid *grid, const TsePressureArgs *args,
+                              TseSolveStatus *d_status, void *stream);
+
 /* Darcy face fluxes, compute_q (tse.py:744-780); the last plane of each
  * component is left untouched as in the reference.  Replaces tse.py:744. */
 int32_t tse_compute_q(const TseGrid *grid, const double *P, const double *BP,

@@ -72,6 +72,7 @@ _PP = ct.POINTER(ct.c_void_p)
 SIGNATURES = {
     "tse_workspace_bytes": (ct.c_size_t, [_G, _I]),
     "tse_compute_P": (_I, [_G, ct.POINTER(TsePressureArgs), _P, _P, _S, _P]),
+    "tse_compute_P_noalloc": (_I, [_G, ct.POINTER(TsePressureArgs), _P, _P]),
     "tse_compute_q": (_I, [_G, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "tse_flow_error": (_I, [_G, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _D, _P, _P]),
     "tse_compute_C": (_I, [_G, ct.POINTER(TseSpeciesArgs), _P, _P, _S, _P]),

@@ -10,6 +10,8 @@
 //                        + Knew - K L + R Pn + WP) / (R + M)       (tse.py:691-695)
 // term by term in the same order, so each cell-update is bit-identical to the
 // reference's.  Compiled with --fmad=false.
+#include <atomic>
+
 #include "tse_rbsolve.cuh"
 
 namespace tse {
@@ -246,4 +248,45 @@ extern "C" int32_t tse_compute_P(const TseGrid* grid, const TsePressureArgs* arg
         args->P, ctl.X[0], ctl.X[1], L);
     if (cudaGetLastError() != cudaSuccess) return TSE_ERR_LAUNCH;
     return TSE_OK;
+}
+
+// ----------------------------------------------------------------------------
+// Pressure solve without any allocation.
+//
+// Some host programs cannot hand this library a workspace: their device
+// memory belongs to an allocator they do not control (a plugin host that
+// passes in only the field buffers, a process held to a fixed memory budget),
+// or their time loop must never stall on cudaMalloc, which can synchronise
+// the whole device.  tse_compute_P_noalloc serves them: its scratch lives in
+// the fixed device array below, which the driver reserves when the library's
+// code is loaded on a GPU and keeps until the process exits.  The array is
+// shared by every call on that GPU, so calls whose execution overlaps on the
+// GPU (different streams, or host threads) corrupt each other; the barrier
+// words the solve needs zeroed are cleared by every call, everything else is
+// rewritten before it is read.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[TSE_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+constexpr int kNoallocMaxDevices = 64;
+std::atomic<void*> g_noalloc_addr[kNoallocMaxDevices];
+}  // namespace
+
+extern "C" int32_t tse_compute_P_noalloc(const TseGrid* grid, const TsePressureArgs* args,
+                                         TseSolveStatus* d_status, void* stream) {
+    if (!grid || !args || !d_status) return TSE_ERR_ARG;
+    if (grid->nx < 1 || grid->ny < 1 || grid->nz < 1) return TSE_ERR_ARG;
+    const Layout L = make_layout(grid->nx, grid->ny, grid->nz);
+    if (pressure_ws_bytes(L, nullptr) > (size_t)TSE_NOALLOC_SCRATCH_BYTES) return TSE_ERR_WORKSPACE;
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kNoallocMaxDevices)
+        return TSE_ERR_DEVICE;
+    void* scratch = g_noalloc_addr[dev].load();
+    if (!scratch) {
+        // first call on this device (the device must be current): host code
+        // only knows the array through its device address
+        if (cudaGetSymbolAddress(&scratch, g_noalloc_scratch) != cudaSuccess || !scratch)
+            return TSE_ERR_DEVICE;
+        g_noalloc_addr[dev].store(scratch);
+    }
+    return tse_compute_P(grid, args, d_status, scratch, (size_t)TSE_NOALLOC_SCRATCH_BYTES, stream);
 }
