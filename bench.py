@@ -1,18 +1,22 @@
 #!/usr/bin/env python
 """Benchmark: SOR cell-updates/s of the TRANSPORTSE time-step core on B200.
 
-Workload (default): the 256 x 256 x 128 bottom-heated reservoir
-(transportse_b200.workloads.reservoir_3d: geometric spacing, GRF log10 K,
-two species plus heat, linear EOS, SIA Picard tolerance 1e-6), synthetic
-seeded inputs.  One step = one full time step of the model (SIA loop with
-pressure solve, fluxes, flow error, species and heat solves, EOS).
+Workload: the 256 x 256 x 128 bottom-heated reservoir
+(transportse_b200.workloads.reservoir_3d: geometric node spacing, Gaussian
+random field log10 K, porosity U(0.05, 0.25), two species plus heat, linear
+EOS, SIA Picard tolerance 1e-6), synthetic seeded inputs.  One step = one
+full time step of the model (SIA loop with pressure solve, fluxes, flow
+error, species and heat solves, EOS).
 
-Metric: cell-updates per second over the timed steps, where a cell-update
-is one active (non-Dirichlet) cell relaxed once in a red+black iteration of
-the pressure, species or heat solve.  ``value`` is measured with all state
-resident in HBM; ``e2e`` repeats the steps through the public API with the
-state uploaded from pinned host memory and the solution read back every
-step.  The working set (~2 GB) is far larger than L2, so no flush is needed.
+Metric: cell-updates per second over the timed steps; a cell-update is one
+active (non-Dirichlet) cell relaxed once in a red+black iteration of the
+pressure, species or heat solve.  The headline ``value`` is the FP32 +
+defect-correction form; the plain FP64 form (the reference's arithmetic) is
+timed on the same inputs and reported beside it, with the largest relative
+difference between the two forms' fields after the same steps.  ``e2e``
+repeats the FP32+DC steps through the public API with the state uploaded
+from pinned host memory and the solution read back every step.  The working
+set (> 3 GB) exceeds L2, so no flush is needed between steps.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 """
@@ -25,13 +29,14 @@ import statistics
 import subprocess
 import sys
 import tempfile
-import threading
 import time
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, HERE)
 
-PRESSURE_BYTES_FP64 = 57   # algorithmic bytes per pressure cell-update, FP64 form
+# algorithmic bytes per pressure cell-update (coefficient form, neighbour
+# reuse from cache): FP64 57 B, FP32 29 B
+ALG_BYTES = {"fp64": 57, "fp32dc": 29}
 DEFAULT_SHAPE = (256, 256, 128)
 
 
@@ -45,6 +50,12 @@ def parse_args():
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--kernel-only", choices=("fp64", "fp32dc"), default=None,
+                    help="time one pressure solve of exactly --iters red+black iterations "
+                         "(for isolated kernel timing and profiler captures)")
+    ap.add_argument("--iters", type=int, default=200)
+    ap.add_argument("--repeat", type=int, default=3)
     return ap.parse_args()
 
 
@@ -55,11 +66,9 @@ def shape_of(a):
 
 
 def measured_peak():
-    p = os.path.join(HERE, "MEASURED_PEAKS.json")
     try:
-        with open(p) as f:
-            d = json.load(f)
-        return float(d["hbm_gbs"]), "measured"
+        with open(os.path.join(HERE, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
 
@@ -127,8 +136,7 @@ def cpu_pressure_rate(shape, seconds):
     cfg = workloads.reservoir_3d(*shape)
     m = O.OracleModel(cfg)
     z = numpy.zeros(shape)
-    rho = numpy.ascontiguousarray(cfg.rho_f)
-    args = (cfg.c_f, cfg.nue, rho, cfg.phi, cfg.Kx, cfg.Ky, cfg.Kz, z, z, z)
+    args = (cfg.c_f, cfg.nue, cfg.rho_f, cfg.phi, cfg.Kx, cfg.Ky, cfg.Kz, z, z, z)
     active = int((cfg.BP == 0).sum())
     P = cfg.P.copy()
     calls, t0 = 0, time.perf_counter()
@@ -150,32 +158,179 @@ def run_reference_arm(a, rank):
     if rank != 0:
         return
     shape = shape_of(a)
-    vals = []
     for _ in range(a.warmup):
         cpu_pressure_rate(shape, 1.0)
-    info = None
+    vals, info = [], None
     for _ in range(a.steps):
         info = cpu_pressure_rate(shape, max(2.0, a.cpu_seconds / max(1, a.steps)))
         vals.append(info["value"])
     v = statistics.mean(vals)
-    line = {"impl": "reference", "metric": "SOR cell-updates/s", "value": v,
-            "unit": "cell-updates/s", "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup,
-            "higher_is_better": True, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "reservoir_3d %dx%dx%d pressure SOR sweeps" % shape},
-            "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": info["cores"],
-                             "kind": info["kind"], "sample": info["sample"]},
-            "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": 0}}
-    print(json.dumps(line))
+    print(json.dumps({
+        "impl": "reference", "metric": "SOR cell-updates/s", "value": v, "unit": "cell-updates/s",
+        "n_gpus": a.gpus, "steps": a.steps, "warmup": a.warmup, "higher_is_better": True,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "reservoir_3d %dx%dx%d pressure SOR sweeps" % shape},
+        "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": info["cores"],
+                         "kind": info["kind"], "sample": info["sample"]},
+        "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0}}))
 
 
 # ---------------------------------------------------------------- GPU arm
+class Ctx:
+    def __init__(self, world, dev):
+        import torch
+        import torch.distributed as dist
+        self.torch, self.dist, self.world, self.dev = torch, dist, world, dev
+
+    def barrier(self):
+        if self.world > 1:
+            self.dist.barrier()
+        self.torch.cuda.synchronize()
+
+    def max_sum(self, ms, units):
+        """(max over ranks of ms, sum over ranks of units)."""
+        t = self.torch.tensor([ms, float(units)], dtype=self.torch.float64, device=self.dev)
+        if self.world > 1:
+            a = t[0:1].clone()
+            b = t[1:2].clone()
+            self.dist.all_reduce(a, op=self.dist.ReduceOp.MAX)
+            self.dist.all_reduce(b, op=self.dist.ReduceOp.SUM)
+            return float(a[0]), float(b[0])
+        return ms, float(units)
+
+
+def timed_steps(ctx, sim, steps, clocks=None):
+    torch = ctx.torch
+    M = sim.M
+    cu0 = dict(M.cell_updates)
+    M.timing, M.timed = True, []
+    launches0 = M.launches
+    if clocks:
+        clocks.start()
+    ctx.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        sim.run(max_steps=1)
+    e1.record()
+    ctx.barrier()
+    clk = clocks.stop() if clocks else None
+    M.timing = False
+    ms = e0.elapsed_time(e1)
+    updates = sum(M.cell_updates[k] - cu0[k] for k in cu0)
+    p_units, p_ms, n_p = 0.0, 0.0, 0
+    for kind, s0, s1, nit, active in M.timed:
+        if kind == "P":
+            p_units += float(nit) * active
+            p_ms += s0.elapsed_time(s1)
+            n_p += 1
+    return {"ms": ms, "updates": updates, "launches": M.launches - launches0, "clocks": clk,
+            "p_units": p_units, "p_ms": p_ms, "n_p": n_p}
+
+
+def e2e_steps(ctx, sim, steps):
+    torch = ctx.torch
+    M = sim.M
+    host = {}
+    for name, tns in sim.S.items():
+        h = torch.empty(tns.shape, dtype=tns.dtype, pin_memory=True)
+        h.copy_(tns)
+        host[name] = h
+    outs = {n: torch.empty(sim.S[n].shape, dtype=torch.float64, pin_memory=True)
+            for n in ("P", "C", "T", "qx", "qy", "qz")}
+    h2d = sum(h.numel() * h.element_size() for h in host.values())
+    d2h = sum(h.numel() * h.element_size() for h in outs.values())
+    cu = dict(M.cell_updates)
+    ctx.barrier()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record()
+    for _ in range(steps):
+        for name, h in host.items():
+            sim.S[name].copy_(h, non_blocking=True)
+        sim.run(max_steps=1)
+        for n, h in outs.items():
+            h.copy_(sim.S[n], non_blocking=True)
+    f1.record()
+    ctx.barrier()
+    ms, upd = ctx.max_sum(f0.elapsed_time(f1), sum(M.cell_updates[k] - cu[k] for k in cu))
+    return {"value": upd / (ms / 1e3), "unit": "cell-updates/s", "h2d_bytes_per_step": int(h2d),
+            "d2h_bytes_per_step": int(d2h)}
+
+
+def roofline(res, precision, peak, peak_kind, traffic=None):
+    if not res["n_p"]:
+        return None
+    achieved = res["p_units"] * ALG_BYTES[precision] / (res["p_ms"] / 1e3) / 1e9
+    name = {"fp32dc": "dc_solve_kernel<PressureForm> (FP32 sweeps + FP64 residual)",
+            "fp64": "rb_solve_kernel<PressureForm> (FP64, reference operation order)"}[precision]
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": traffic, "kernel": name,
+            "algorithmic_bytes_per_cell_update": ALG_BYTES[precision],
+            "cell_updates_per_launch": res["p_units"] / res["n_p"],
+            "peak_source": peak_kind, "launches": res["n_p"]}
+
+
+def load_traffic(precision):
+    """DRAM bytes per cell-update of the pressure kernel from the committed ncu
+    summary (profiles/traffic.json), scaled to one launch by the caller."""
+    try:
+        with open(os.path.join(HERE, "profiles", "traffic.json")) as f:
+            return json.load(f).get(precision)
+    except Exception:
+        return None
+
+
+def kernel_only(a):
+    """One pressure solve of exactly a.iters iterations (P_conv = 0, so it
+    never converges; max_it = a.iters and min_dt = dt, so the first dt halving
+    ends it), repeated a.repeat times; prints per-launch time and bandwidth."""
+    import torch
+    from transportse_b200 import workloads
+    from transportse_b200.driver import Simulation
+    shape = shape_of(a)
+    sim = Simulation(workloads.reservoir_3d(*shape), device=torch.device("cuda:0"),
+                     precision=a.kernel_only)
+    M, S = sim.M, sim.S
+    M.dc_min_conv = 0.0   # P_conv = 0 below: keep the requested form
+    P0 = S["P"].clone()
+    peak, kind = measured_peak()
+    out = []
+    for r in range(a.repeat + 1):
+        S["P"].copy_(P0)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        res = M.compute_P(S["P"], S["c_f"], S["nue"], S["rho_f"], S["phi"], S["Kx"], S["Ky"],
+                          S["Kz"], S["qx"], S["qy"], S["qz"], 3600.0, S["BP"], S["WP"],
+                          SOR=1.9, max_it=a.iters, inc_it=1.25, max_dt=1e6, min_dt=2700.0,
+                          P_conv=0.0)
+        e1.record()
+        torch.cuda.synchronize()
+        if r:
+            out.append((e0.elapsed_time(e1), res[5]))
+    active = int((S["BP"] == 0).sum().item())
+    ms = statistics.median(x[0] for x in out)
+    its = out[0][1]
+    rate = its * active / (ms / 1e3)
+    st = M.last_status
+    print(json.dumps({"kernel_only": a.kernel_only, "shape": list(shape), "iterations": its,
+                      "residual_cycles": int(st.cycles), "halvings": int(st.halvings),
+                      "ms_per_launch": ms, "cell_updates_per_s": rate,
+                      "alg_GBps": rate * ALG_BYTES[a.kernel_only] / 1e9,
+                      "frac_of_peak": rate * ALG_BYTES[a.kernel_only] / 1e9 / peak,
+                      "peak_GBps": peak, "peak_source": kind}))
+
+
 def main():
     a = parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if a.impl == "reference":
         return run_reference_arm(a, rank)
+    if a.kernel_only:
+        return kernel_only(a)
+    import numpy
     import torch
     import torch.distributed as dist
     from transportse_b200 import workloads
@@ -185,118 +340,58 @@ def main():
     dev = torch.device("cuda", local)
     if world > 1:
         import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
-                                device_id=dev)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600), device_id=dev)
+    ctx = Ctx(world, dev)
     shape = shape_of(a)
-    cfg = workloads.reservoir_3d(*shape)
-    sim = Simulation(cfg, device=dev)
-    M = sim.M
+    peak, peak_kind = measured_peak()
+
+    # ---- headline: FP32 sweeps + FP64 defect correction
+    sim = Simulation(workloads.reservoir_3d(*shape), device=dev, precision="fp32dc")
     for _ in range(a.warmup):
         sim.run(max_steps=1)
-    torch.cuda.synchronize()
+    res = timed_steps(ctx, sim, a.steps, ClockSampler(local))
+    ms, upd = ctx.max_sum(res["ms"], res["updates"])
+    value = upd / (ms / 1e3)
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    # ---------------- device-resident timed region
-    cu0 = dict(M.cell_updates)
-    M.timing = True
-    M.timed = []
-    launches0 = M.launches
-    clocks = ClockSampler(local)
-    clocks.start()
-    barrier()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(a.steps):
-        sim.run(max_steps=1)
-    e1.record()
-    barrier()
-    clk = clocks.stop()
-    M.timing = False
-    ms = e0.elapsed_time(e1)
-    updates = sum(M.cell_updates[k] - cu0[k] for k in cu0)
-    gpu_launches = M.launches - launches0
-    # pressure-solve launches: algorithmic bytes / event duration
-    p_bytes, p_ms, n_p = 0.0, 0.0, 0
-    for kind, s0, s1, nit, active in M.timed:
-        if kind == "P":
-            p_bytes += float(nit) * active * PRESSURE_BYTES_FP64
-            p_ms += s0.elapsed_time(s1)
-            n_p += 1
-    t = torch.tensor([ms, float(updates)], dtype=torch.float64, device=dev)
-    if world > 1:
-        tmax = t.clone()
-        dist.all_reduce(tmax[0:1], op=dist.ReduceOp.MAX)
-        dist.all_reduce(t[1:2], op=dist.ReduceOp.SUM)
-        ms_max, upd_all = float(tmax[0]), float(t[1])
-    else:
-        ms_max, upd_all = ms, float(updates)
-    value = upd_all / (ms_max / 1e3)
-
-    # ---------------- end-to-end through the public API with host buffers
-    e2e = None
-    if not a.no_e2e:
-        host = {}
-        for name, tns in sim.S.items():
-            h = torch.empty(tns.shape, dtype=tns.dtype, pin_memory=True)
-            h.copy_(tns)
-            host[name] = h
-        outs = {n: torch.empty(sim.S[n].shape, dtype=torch.float64, pin_memory=True)
-                for n in ("P", "C", "T", "qx", "qy", "qz")}
-        h2d = sum(h.numel() * h.element_size() for h in host.values())
-        d2h = sum(h.numel() * h.element_size() for h in outs.values())
-        cu1 = dict(M.cell_updates)
-        barrier()
-        f0 = torch.cuda.Event(enable_timing=True)
-        f1 = torch.cuda.Event(enable_timing=True)
-        f0.record()
-        for _ in range(a.steps):
-            for name, h in host.items():
-                sim.S[name].copy_(h, non_blocking=True)
-            sim.run(max_steps=1)
-            for n, h in outs.items():
-                h.copy_(sim.S[n], non_blocking=True)
-        f1.record()
-        barrier()
-        ms_e2e = f0.elapsed_time(f1)
-        upd_e2e = sum(M.cell_updates[k] - cu1[k] for k in cu1)
-        te = torch.tensor([ms_e2e, float(upd_e2e)], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(te[0:1], op=dist.ReduceOp.MAX)
-            tsum = torch.tensor([float(upd_e2e)], dtype=torch.float64, device=dev)
-            dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
-            te[1] = tsum[0]
-        e2e = {"value": float(te[1]) / (float(te[0]) / 1e3), "unit": "cell-updates/s",
-               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}
-
-    peak, peak_kind = measured_peak()
-    roof = None
-    if n_p:
-        achieved = p_bytes / (p_ms / 1e3) / 1e9
-        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": None,
-                "kernel": "rb_solve_kernel<PressureForm> (FP64 exact, per compute_P launch)",
-                "algorithmic_bytes_per_cell_update": PRESSURE_BYTES_FP64,
-                "peak_source": peak_kind, "launches": n_p}
+    # ---- the plain FP64 form on the same inputs and steps
+    fp64 = None
+    if not a.no_fp64:
+        sim64 = Simulation(workloads.reservoir_3d(*shape), device=dev, precision="fp64")
+        for _ in range(a.warmup):
+            sim64.run(max_steps=1)
+        r64 = timed_steps(ctx, sim64, a.steps)
+        ms64, upd64 = ctx.max_sum(r64["ms"], r64["updates"])
+        err = {}
+        for n in ("P", "C", "T"):
+            x, y = sim.field(n), sim64.field(n)
+            err[n] = float(numpy.max(numpy.abs(x - y)) / max(numpy.max(numpy.abs(y)), 1e-300))
+        fp64 = {"value": upd64 / (ms64 / 1e3), "ms_per_step": ms64 / a.steps,
+                "speedup_fp32dc": value / (upd64 / (ms64 / 1e3)),
+                "step_time_ratio": (ms64 / a.steps) / (ms / a.steps),
+                "max_rel_err_vs_fp64": err,
+                "roofline": roofline(r64, "fp64", peak, peak_kind)}
+        del sim64
+        torch.cuda.empty_cache()
+    e2e = None if a.no_e2e else e2e_steps(ctx, sim, a.steps)
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
         cpu = cpu_pressure_rate(shape, a.cpu_seconds)
+    tr = load_traffic("fp32dc")
+    roof = roofline(res, "fp32dc", peak, peak_kind)
+    if roof and tr:
+        roof["traffic"] = tr * roof["cell_updates_per_launch"]
     if rank == 0:
-        line = {"metric": "SOR cell-updates/s", "value": value, "unit": "cell-updates/s",
-                "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
-                "ms_per_step": ms_max / a.steps, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": "reservoir_3d %dx%dx%d, full time steps (SIA loop), "
-                                       "FP64 plain form" % shape,
-                           "parallelism": "replicas" if world > 1 else "single",
-                           "l2": "working set > L2 (no flush)"},
-                "gpu_launches": int(gpu_launches), "clocks": clk, "e2e": e2e,
-                "roofline": roof, "cpu_baseline": cpu}
-        print(json.dumps(line))
+        print(json.dumps({
+            "metric": "SOR cell-updates/s", "value": value, "unit": "cell-updates/s",
+            "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": ms / a.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": "reservoir_3d %dx%dx%d, full time steps (SIA loop), "
+                                   "FP32 sweeps + FP64 defect correction" % shape,
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "working set > L2 (no flush)"},
+            "gpu_launches": int(res["launches"]), "clocks": res["clocks"], "e2e": e2e,
+            "roofline": roof, "fp64_plain": fp64, "cpu_baseline": cpu}))
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

@@ -72,6 +72,8 @@ typedef struct TseSolveStatus {
     int32_t ev_it[8];
     double ev_dt[8];
     double ev_diff[8];
+    int32_t cycles;    /* mixed-precision forms: FP64 residual evaluations */
+    int32_t reserved;
 } TseSolveStatus;
 
 /* Pressure solve arguments, compute_P(P, c_f, nue, rho_f, phi, Kx, Ky, Kz,
@@ -114,6 +116,8 @@ typedef struct TseHeatArgs {
 #define TSE_WS_PRESSURE 1
 #define TSE_WS_TRANSPORT 2
 #define TSE_WS_REDUCE 3
+#define TSE_WS_PRESSURE_DC 4
+#define TSE_WS_TRANSPORT_DC 5
 
 /* Bytes of device workspace a call of the given kind needs for this grid. */
 size_t tse_workspace_bytes(const TseGrid *grid, int32_t kind);
@@ -124,6 +128,26 @@ size_t tse_workspace_bytes(const TseGrid *grid, int32_t kind);
 int32_t tse_compute_P(const TseGrid *grid, const TsePressureArgs *args,
                       TseSolveStatus *d_status, void *d_workspace,
                       size_t workspace_bytes, void *stream);
+
+/* Mixed-precision forms of compute_P / compute_C / compute_T (tse.py:647,
+ * 783, 919): the FP64 residual of the reference's per-cell equation drives
+ * red-black SOR sweeps on an FP32 correction, which is added to the FP64
+ * iterate every `cycle` iterations (<= 0: 128) and at convergence.  Same
+ * arguments, convergence test, dt control and results as the FP64 entry
+ * points; agreement with them is to the solver tolerance, not bit for bit.
+ * Workspace: TSE_WS_PRESSURE_DC / TSE_WS_TRANSPORT_DC. */
+int32_t tse_compute_P_dc(const TseGrid *grid, const TsePressureArgs *args,
+                         int32_t cycle, TseSolveStatus *d_status,
+                         void *d_workspace, size_t workspace_bytes,
+                         void *stream);
+int32_t tse_compute_C_dc(const TseGrid *grid, const TseSpeciesArgs *args,
+                         int32_t cycle, TseSolveStatus *d_status,
+                         void *d_workspace, size_t workspace_bytes,
+                         void *stream);
+int32_t tse_compute_T_dc(const TseGrid *grid, const TseHeatArgs *args,
+                         int32_t cycle, TseSolveStatus *d_status,
+                         void *d_workspace, size_t workspace_bytes,
+                         void *stream);
 
 /* Pressure solve that allocates nothing and takes no workspace.  It has no
  * counterpart in the reference; it exists for callers that cannot allocate

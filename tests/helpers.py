@@ -69,9 +69,9 @@ class NumpyKernels:
         return self.m.l2_norm(*a, **k)
 
 
-def model_for(cfg, device):
+def model_for(cfg, device, precision="fp64"):
     from transportse_b200.kernels import Model
-    m = Model.from_config(cfg, device=device)
+    m = Model.from_config(cfg, device=device, precision=precision)
     m.freeze(cfg.c_r, cfg.l_r, cfg.rho_r, cfg.cp_r, cfg.lf_l, cfg.lf_t, cfg.lt_l, cfg.lt_t,
              cfg.C_IMBLFLO, cfg.T_IMBLFLO)
     return m

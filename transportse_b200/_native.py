@@ -15,6 +15,8 @@ LIB_PATH = os.path.join(_HERE, "_build", "libtsecuda.so")
 TSE_WS_PRESSURE = 1
 TSE_WS_TRANSPORT = 2
 TSE_WS_REDUCE = 3
+TSE_WS_PRESSURE_DC = 4
+TSE_WS_TRANSPORT_DC = 5
 
 ERRORS = {-1: "invalid argument", -2: "workspace too small", -3: "kernel launch failed",
           -4: "device error"}
@@ -34,7 +36,7 @@ class TseSolveStatus(ct.Structure):
                 ("converged", ct.c_int32), ("num_it", ct.c_int32), ("num_sub_it", ct.c_int32),
                 ("halvings", ct.c_int32), ("error", ct.c_int32), ("n_events", ct.c_int32),
                 ("ev_it", ct.c_int32 * 8), ("ev_dt", ct.c_double * 8),
-                ("ev_diff", ct.c_double * 8)]
+                ("ev_diff", ct.c_double * 8), ("cycles", ct.c_int32), ("reserved", ct.c_int32)]
 
 
 def _ptr_fields(names):
@@ -73,6 +75,9 @@ SIGNATURES = {
     "tse_workspace_bytes": (ct.c_size_t, [_G, _I]),
     "tse_compute_P": (_I, [_G, ct.POINTER(TsePressureArgs), _P, _P, _S, _P]),
     "tse_compute_P_noalloc": (_I, [_G, ct.POINTER(TsePressureArgs), _P, _P]),
+    "tse_compute_P_dc": (_I, [_G, ct.POINTER(TsePressureArgs), _I, _P, _P, _S, _P]),
+    "tse_compute_C_dc": (_I, [_G, ct.POINTER(TseSpeciesArgs), _I, _P, _P, _S, _P]),
+    "tse_compute_T_dc": (_I, [_G, ct.POINTER(TseHeatArgs), _I, _P, _P, _S, _P]),
     "tse_compute_q": (_I, [_G, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "tse_flow_error": (_I, [_G, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _D, _P, _P]),
     "tse_compute_C": (_I, [_G, ct.POINTER(TseSpeciesArgs), _P, _P, _S, _P]),

@@ -30,6 +30,7 @@ SOURCES = {
     "tse_transport.cu": ["--fmad=false"],
     "tse_flow.cu": ["--fmad=false"],
     "tse_capi.cu": ["--fmad=false"],
+    "tse_dc.cu": [],
 }
 
 

@@ -1,0 +1,498 @@
+// FP32 red-black SOR with FP64 defect correction: the mixed-precision form of
+// the pressure, species and heat solves.
+//
+// The FP64 solves (tse_pressure.cu, tse_transport.cu) stream 11-15 double
+// words per cell-update.  Here the same SOR iteration runs on a correction:
+// with the FP64 iterate x, the residual of the reference's per-cell equation
+//   r = sum(x) - Den * x            (sum / Den as in compute_P/C/T.solve)
+// is formed in FP64, and red-black SOR sweeps
+//   d = (1 - SOR) d + SOR (sum_q K'_q d_q + r')  with K'_q = k_q / Den, r' = r / Den
+// run in FP32 from d = 0.  In exact arithmetic x + d follows the FP64 SOR
+// iteration step for step, so the reference's convergence test (relative L2
+// change of one iteration, checked on its schedule) and its dt control are
+// applied to the change of d unchanged.  x += d in FP64 and the residual is
+// formed again (a correction cycle ends) at convergence, every `cycle`
+// iterations, and at a check whose change has fallen below kRefresh * |d|:
+// FP32 resolves d to ~6e-8 |d|, so the measured change stays ~1e3 times above
+// d's rounding and the iteration counts track the FP64 form's.
+//
+// Kernels: the FP32 sweeps run in one cooperative kernel that iterates until
+// an event (converged, cycle end, dt halving, stop); it needs ~40 registers,
+// so 6 blocks fit per SM.  The FP64 residual, the x += d update and the dt
+// halving (reset + new R terms) are separate, ordinary kernels, so their
+// register appetite does not limit the sweeps' occupancy.  The host reads one
+// small state record per correction cycle.
+//
+// An inner cell-update streams the six FP32 coefficients (one 24-byte record),
+// r', the flag byte and d (read + write) plus the neighbours' d: ~37 bytes
+// against 113-129 for the FP64 form.
+//
+// Compiled with FMA contraction (no bit-exactness is claimed for this form).
+#include "tse_forms.cuh"
+#include "tse_rbsolve.cuh"
+
+namespace tse {
+
+constexpr double kRefresh = 1e-4;
+#ifndef TSE_SWEEP_MINB
+#define TSE_SWEEP_MINB 5   // 48 registers, no spills (measured best of 4/5/6/8)
+#endif
+constexpr int kSweepMinBlocks = TSE_SWEEP_MINB;
+constexpr int kResBlocks = 2048;   // fixed grid of the residual kernel (deterministic sums)
+
+// events that end a sweep launch
+enum DcEvent { EV_NONE = 0, EV_CONVERGED, EV_CYCLE_END, EV_REFRESH, EV_HALVE, EV_STOP,
+               EV_STOP_HALVED, EV_ERROR };
+
+// Solver state carried across the kernels of one solve (device memory).
+struct DcState {
+    double t, dt, diff, x2;
+    int num_it, num_sub_it, halvings, converged;
+    int event, nev, cycles, checkno;
+    int ev_it[8];
+    double ev_dt[8];
+    double ev_diff[8];
+};
+
+struct DcCtl {
+    Layout L;
+    long long Ncal;
+    double inc_it, max_dt, min_dt, conv;
+    int max_it;
+    int pressure_schedule;
+    int stop_on_first;
+    int cycle;           // inner iterations between residual updates
+    float sor;
+    double* X[2];        // FP64 iterate per colour
+    const uint8_t* mask[2];
+    float* K[2];         // per colour: Ncal 24-byte coefficient records, then Ncal r'
+    float* D[2];         // per colour: correction, valid on [-G, Nc + G); the
+                         // margins stay 0 so neighbour loads need no guard
+    double* partials;    // sweep kernel: 4 per block; residual kernel: 1 per block
+    GridBarrier* bar;
+    DcState* st;
+};
+
+// ------------------------------------------------------------ FP64 kernels
+template <class Form>
+__device__ __forceinline__ void scale_cell(const Form& F, const DcCtl& c, int col, long long m) {
+    float2* rec = reinterpret_cast<float2*>(c.K[col] + 6 * m);
+    if (c.mask[col][m] & F_ACTIVE) {
+        const double den = F.den(col, m);
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+            rec[q] = make_float2((float)(F.k(col, m, 2 * q) / den), (float)(F.k(col, m, 2 * q + 1) / den));
+    } else {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) rec[q] = make_float2(0.0f, 0.0f);
+    }
+}
+
+// K'_q = k_q / Den for every cell (at the start and after dt halving)
+template <class Form>
+__global__ void dc_scale_kernel(Form F, DcCtl c) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 2 * c.L.Nc) return;
+    const int col = t >= c.L.Nc;
+    scale_cell(F, c, col, t - col * c.L.Nc);
+}
+
+// dt halving: x = Xn, new R terms (tse.py:733-738), rescaled coefficients
+template <class Form>
+__global__ void dc_halve_kernel(Form F, DcCtl c) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 2 * c.L.Nc) return;
+    const int col = t >= c.L.Nc;
+    const long long m = t - col * c.L.Nc;
+    F.reassemble(col, m, c.st->dt);
+    scale_cell(F, c, col, m);
+}
+
+// r' = (sum(x) - Den x) / Den in FP64, d = 0, per-block sums of x^2
+template <class Form>
+__global__ void __launch_bounds__(kBlock) dc_residual_kernel(Form F, DcCtl c) {
+    __shared__ double sh[kBlock / 32];
+    const long long Nc = c.L.Nc;
+    double o2 = 0.0;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < 2 * Nc;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int col = t >= Nc;
+        const long long m = t - col * Nc;
+        const uint8_t f = c.mask[col][m];
+        const double x = c.X[col][m];
+        o2 = o2 + x * x;
+        float rp = 0.0f;
+        if (f & F_ACTIVE) {
+            const double den = F.den(col, m);
+            const double r = F.sum(col, m, f, c.X[1 - col]) - den * x;
+            rp = (float)(r / den);
+        }
+        c.K[col][6 * c.Ncal + m] = rp;
+        c.D[col][m] = 0.0f;
+    }
+    const double b = block_sum<kBlock>(o2, sh);
+    if (threadIdx.x == 0) c.partials[blockIdx.x] = b;
+}
+
+// x^2 total into the state; counts the cycle
+__global__ void dc_x2_kernel(DcCtl c, int nparts) {
+    __shared__ double sh[kBlock / 32];
+    double s = 0.0;
+    for (int b = threadIdx.x; b < nparts; b += blockDim.x) s = s + c.partials[b];
+    s = block_sum<kBlock>(s, sh);
+    if (threadIdx.x == 0) {
+        c.st->x2 = s;
+        c.st->cycles += 1;
+    }
+}
+
+// x += d for active cells
+__global__ void dc_apply_kernel(DcCtl c) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 2 * c.L.Nc) return;
+    const int col = t >= c.L.Nc;
+    const long long m = t - col * c.L.Nc;
+    if (c.mask[col][m] & F_ACTIVE) c.X[col][m] = c.X[col][m] + (double)c.D[col][m];
+}
+
+// ------------------------------------------------------------ FP32 sweeps
+// The coefficients of a cell are one 24-byte record (three 8-byte loads
+// from one address); the z-neighbours dq[m-1], dq[m+1] are the dq[m] values
+// the adjacent lanes load (consecutive lanes hold consecutive m), fetched
+// from memory only at a warp's edge or the end of the range.  All lanes of a
+// warp call relax() together.
+struct Cell {
+    float2 k01, k23, k45;
+    float r, old, xp, xm, yp, ym, z1;
+    bool odd;
+};
+
+__device__ __forceinline__ void load_cell(Cell& a, const float* __restrict__ Kc, const float* dw,
+                                          const float* dq, const uint8_t* __restrict__ msk,
+                                          long long m, long long N, long long SX, int H) {
+    const float2* rec = reinterpret_cast<const float2*>(Kc + 6 * m);
+    a.k01 = rec[0];
+    a.k23 = rec[1];
+    a.k45 = rec[2];
+    a.r = Kc[6 * N + m];
+    a.odd = (msk[m] & F_KODD) != 0;
+    a.old = dw[m];
+    a.xp = __ldcg(dq + m + SX);
+    a.xm = __ldcg(dq + m - SX);
+    a.yp = __ldcg(dq + m + H);
+    a.ym = __ldcg(dq + m - H);
+    a.z1 = __ldcg(dq + m);
+}
+
+__device__ __forceinline__ float relax(const Cell& a, const float* dq, long long m, long long end,
+                                       float sor) {
+    const int lane = threadIdx.x & 31;
+    float z0 = __shfl_up_sync(0xffffffffu, a.z1, 1);
+    float z2 = __shfl_down_sync(0xffffffffu, a.z1, 1);
+    if (lane == 0) z0 = __ldcg(dq + m - 1);
+    if (lane == 31 || m + 1 >= end) z2 = __ldcg(dq + m + 1);
+    float acc = a.r;
+    acc = fmaf(a.k01.x, a.xp, acc);
+    acc = fmaf(a.k01.y, a.xm, acc);
+    acc = fmaf(a.k23.x, a.yp, acc);
+    acc = fmaf(a.k23.y, a.ym, acc);
+    acc = fmaf(a.k45.x, a.odd ? z2 : a.z1, acc);
+    acc = fmaf(a.k45.y, a.odd ? a.z1 : z0, acc);
+    return fmaf(sor, acc - a.old, a.old);
+}
+
+__device__ __forceinline__ double reduce_slot(const double* parts, int slot, unsigned nb, double* sh,
+                                              double* s_val) {
+    double s = 0.0;
+    for (unsigned b = threadIdx.x; b < nb; b += blockDim.x) s = s + __ldcg(parts + 4 * b + slot);
+    s = block_sum<kBlock>(s, sh);
+    if (threadIdx.x == 0) *s_val = s;
+    __syncthreads();
+    const double r = *s_val;
+    __syncthreads();
+    return r;
+}
+
+// Inner iterations of one correction cycle.  Cells are interleaved over the
+// grid (block b, thread t: m = b*256 + t + s*gridDim*256), which keeps all
+// blocks streaming one narrow window of memory; colour phases are separated
+// by the grid barrier.  Per-block partial sums alternate between two slot
+// pairs by check parity, so a slot is rewritten only after a further barrier.
+__global__ void __launch_bounds__(kBlock, kSweepMinBlocks) dc_sweep_kernel(DcCtl c) {
+    __shared__ double sh[kBlock / 32];
+    __shared__ double s_val;
+    const unsigned nb = gridDim.x;
+    const long long Nc = c.L.Nc, N = c.Ncal, SX = c.L.SX;
+    const int H = c.L.H;
+    const long long step = (long long)nb * blockDim.x;
+    const int lane = threadIdx.x & 31;
+    const long long w0 = (long long)blockIdx.x * blockDim.x + threadIdx.x - lane;
+    const bool leader = (blockIdx.x == 0 && threadIdx.x == 0);
+    const float sor = c.sor;
+    DcState* st = c.st;
+    double t = st->t, dt = st->dt, diff = 1e100;
+    const double x2 = st->x2;
+    int num_it = st->num_it, num_sub_it = st->num_sub_it, checkno = st->checkno;
+    int event = EV_CYCLE_END;
+    bool halved = false;
+
+    for (int inner = 0; inner < c.cycle; ++inner) {
+        num_it += 1;
+        num_sub_it += 1;
+        const bool check = c.pressure_schedule ? (num_it < 50 || num_it % 10 == 0) : true;
+        if (check) checkno += 1;
+        float d2 = 0.0f, dd = 0.0f;
+        bool ok = true;
+        for (int col = 0; col < 2 && ok; ++col) {
+            const float* __restrict__ Kc = c.K[col];
+            float* dw = c.D[col];
+            const float* dq = c.D[1 - col];
+            const uint8_t* __restrict__ msk = c.mask[col];
+            // all loads of a cell are independent: coefficients of absent
+            // neighbours are 0 and dq's margins are 0; inactive cells have
+            // all-zero coefficients and r' = 0 and stay at d = 0.  Trips are
+            // counted per warp so every lane joins the shuffles; lanes past
+            // the end load a valid cell and store nothing.
+            for (long long w = w0; w < Nc; w += step) {
+                const long long ma = w + lane;
+                const bool va = ma < Nc;
+                const long long la = va ? ma : Nc - 1;
+                Cell a;
+                load_cell(a, Kc, dw, dq, msk, la, N, SX, H);
+                const float na = relax(a, dq, la, Nc, sor);
+                if (va) {
+                    dw[ma] = na;
+                    const float ch = na - a.old;
+                    d2 = fmaf(ch, ch, d2);
+                    dd = fmaf(na, na, dd);
+                }
+            }
+            if (col == 1 && check) {
+                const double b1 = block_sum<kBlock>((double)d2, sh);
+                const double b3 = block_sum<kBlock>((double)dd, sh);
+                if (threadIdx.x == 0) {
+                    c.partials[4 * blockIdx.x + 2 * (checkno & 1)] = b1;
+                    c.partials[4 * blockIdx.x + 2 * (checkno & 1) + 1] = b3;
+                }
+            }
+            ok = grid_sync(c.bar, nb);
+        }
+        if (!ok) { event = EV_ERROR; break; }
+        diff = 1e100;
+        bool refresh = false;
+        if (check) {
+            const double s1 = reduce_slot(c.partials, 2 * (checkno & 1), nb, sh, &s_val);
+            const double s3 = reduce_slot(c.partials, 2 * (checkno & 1) + 1, nb, sh, &s_val);
+            const double l2 = sqrt(s1) / sqrt(x2 + 1e-200);
+            diff = (l2 != l2) ? 1.0 : l2;
+            refresh = sqrt(s1) < kRefresh * sqrt(s3);
+        }
+        if (diff < c.conv || c.stop_on_first) {
+            t += dt;
+            if (num_sub_it < c.max_it / 2.0) dt = pymin(dt * c.inc_it, c.max_dt);
+            event = EV_CONVERGED;
+            break;
+        }
+        if (num_sub_it >= c.max_it) {
+            if (leader && st->nev < 8) {
+                st->ev_it[st->nev] = num_it;
+                st->ev_dt[st->nev] = dt;
+                st->ev_diff[st->nev] = diff;
+            }
+            if (leader) st->nev += 1;
+            dt = dt / 2;
+            num_sub_it = 0;
+            halved = true;
+        }
+        if (dt <= c.min_dt) { event = halved ? EV_STOP_HALVED : EV_STOP; break; }
+        if (halved) { event = EV_HALVE; break; }
+        if (refresh) { event = EV_REFRESH; break; }
+    }
+    if (leader) {
+        st->t = t;
+        st->dt = dt;
+        st->diff = diff;
+        st->num_it = num_it;
+        st->num_sub_it = num_sub_it;
+        st->checkno = checkno;
+        st->event = event;
+        if (halved) st->halvings += 1;
+        if (event == EV_CONVERGED) st->converged = 1;
+    }
+}
+
+// copy the final state into the caller's status record
+__global__ void dc_status_kernel(const DcState* st, TseSolveStatus* s) {
+    s->t = st->t;
+    s->dt = st->dt;
+    s->diff = st->diff;
+    s->converged = st->converged;
+    s->num_it = st->num_it;
+    s->num_sub_it = st->num_sub_it;
+    s->halvings = st->halvings;
+    s->error = st->event == EV_ERROR ? TSE_STATUS_BARRIER_TIMEOUT : TSE_STATUS_OK;
+    s->n_events = st->nev < 8 ? st->nev : 8;
+    for (int q = 0; q < 8; ++q) {
+        s->ev_it[q] = st->ev_it[q];
+        s->ev_dt[q] = st->ev_dt[q];
+        s->ev_diff[q] = st->ev_diff[q];
+    }
+    s->cycles = st->cycles;
+}
+
+// ------------------------------------------------------------------ host
+// FP32 arrays: per colour 7 * Ncal floats (records + r'), then the
+// correction with margins of G >= SX + 1, then the state record
+static long long dc_margin(const Layout& L) { return ((L.SX + 1 + 63) / 64) * 64; }
+static long long dc_delta_len(const Layout& L, long long Ncal) { return Ncal + 2 * dc_margin(L); }
+
+size_t dc_extra_bytes(const Layout& L) {
+    long long Ncal = (L.Nc + 31) & ~31LL;
+    return 2 * ((size_t)7 * Ncal + (size_t)dc_delta_len(L, Ncal)) * sizeof(float) +
+           align256(sizeof(DcState)) + 512;
+}
+
+static int sweep_blocks(long long Nc) {
+    static int cached_dev = -1, cached_per_sm = 0, cached_sms = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev != cached_dev) {
+        cudaDeviceGetAttribute(&cached_sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cached_per_sm, dc_sweep_kernel, kBlock, 0);
+        cached_dev = dev;
+    }
+    long long maxb = (long long)cached_sms * (cached_per_sm > 0 ? cached_per_sm : 1);
+    long long want = (Nc + (long long)kBlock * 4 - 1) / ((long long)kBlock * 4);
+    if (want < 1) want = 1;
+    long long nb = want < maxb ? want : maxb;
+    // the setup's partials region holds 2 * kMaxBlocks doubles
+    if (nb > kMaxBlocks / 2) nb = kMaxBlocks / 2;
+    return (int)nb;
+}
+
+template <class Form>
+static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, double min_dt,
+                  double conv, int max_it, int pressure_schedule, int stop_on_first, int cycle,
+                  double sor, int x_index, double* X_out, TseSolveStatus* d_status,
+                  cudaStream_t stream) {
+    if (S.tail_bytes < dc_extra_bytes(S.L)) return TSE_ERR_WORKSPACE;
+    DcCtl c;
+    c.L = S.L;
+    c.Ncal = S.Ncal;
+    c.inc_it = inc_it;
+    c.max_dt = max_dt;
+    c.min_dt = min_dt;
+    c.conv = conv;
+    c.max_it = max_it;
+    c.pressure_schedule = pressure_schedule;
+    c.stop_on_first = stop_on_first;
+    c.cycle = cycle > 0 ? cycle : 128;
+    c.sor = (float)sor;
+    c.X[0] = S.F.arr[0] + (size_t)x_index * S.Ncal;
+    c.X[1] = S.F.arr[1] + (size_t)x_index * S.Ncal;
+    c.mask[0] = S.mask[0];
+    c.mask[1] = S.mask[1];
+    float* base = (float*)(((uintptr_t)S.tail + 255) & ~(uintptr_t)255);
+    const long long G = dc_margin(S.L), dlen = dc_delta_len(S.L, S.Ncal);
+    c.K[0] = base;
+    c.K[1] = base + (size_t)7 * S.Ncal;
+    float* dbase = base + (size_t)14 * S.Ncal;
+    c.D[0] = dbase + G;
+    c.D[1] = dbase + dlen + G;
+    c.st = (DcState*)(dbase + 2 * dlen);
+    c.partials = S.partials;
+    c.bar = S.bar;
+    DcState init;
+    memset(&init, 0, sizeof(init));
+    init.dt = dt;
+    init.diff = 1e100;
+    // the margins must read as 0 (kernels rewrite the interior only)
+    if (cudaMemsetAsync(dbase, 0, (size_t)2 * dlen * sizeof(float), stream) != cudaSuccess ||
+        cudaMemcpyAsync(c.st, &init, sizeof(DcState), cudaMemcpyHostToDevice, stream) != cudaSuccess)
+        return TSE_ERR_LAUNCH;
+    const long long cells2 = 2 * S.L.Nc;
+    const unsigned gcells = (unsigned)((cells2 + kBlock - 1) / kBlock);
+    const int nb = sweep_blocks(S.L.Nc);
+    dc_scale_kernel<<<gcells, kBlock, 0, stream>>>(S.F, c);
+    if (cudaGetLastError() != cudaSuccess) return TSE_ERR_LAUNCH;
+    for (;;) {
+        const unsigned rb = (unsigned)std::min<long long>(kResBlocks, (cells2 + kBlock - 1) / kBlock);
+        dc_residual_kernel<<<rb, kBlock, 0, stream>>>(S.F, c);
+        dc_x2_kernel<<<1, kBlock, 0, stream>>>(c, (int)rb);
+        void* args[] = {(void*)&c};
+        if (cudaGetLastError() != cudaSuccess ||
+            cudaLaunchCooperativeKernel((const void*)dc_sweep_kernel, dim3(nb), dim3(kBlock), args, 0,
+                                        stream) != cudaSuccess)
+            return TSE_ERR_LAUNCH;
+        int event = EV_ERROR;
+        if (cudaMemcpyAsync(&event, &c.st->event, sizeof(int), cudaMemcpyDeviceToHost, stream) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(stream) != cudaSuccess)
+            return TSE_ERR_LAUNCH;
+        if (event == EV_HALVE || event == EV_STOP_HALVED) {
+            dc_halve_kernel<<<gcells, kBlock, 0, stream>>>(S.F, c);
+            if (cudaGetLastError() != cudaSuccess) return TSE_ERR_LAUNCH;
+            if (event == EV_STOP_HALVED) break;
+            continue;
+        }
+        if (event == EV_ERROR) break;
+        dc_apply_kernel<<<gcells, kBlock, 0, stream>>>(c);
+        if (cudaGetLastError() != cudaSuccess) return TSE_ERR_LAUNCH;
+        if (event == EV_CONVERGED || event == EV_STOP) break;
+    }
+    dc_status_kernel<<<1, 1, 0, stream>>>(c.st, d_status);
+    if (cudaGetLastError() != cudaSuccess) return TSE_ERR_LAUNCH;
+    return launch_unpack(X_out, c.X[0], c.X[1], S.L, stream);
+}
+
+}  // namespace tse
+
+using namespace tse;
+
+extern "C" int32_t tse_compute_P_dc(const TseGrid* grid, const TsePressureArgs* args, int32_t cycle,
+                                    TseSolveStatus* d_status, void* d_ws, size_t ws_bytes,
+                                    void* stream_) {
+    if (!grid || !args || !d_status || !d_ws) return TSE_ERR_ARG;
+    if (grid->nx < 1 || grid->ny < 1 || grid->nz < 1 || args->max_it < 1) return TSE_ERR_ARG;
+    if (!args->P || !args->Pn || !args->c_f || !args->nue || !args->rho_f || !args->phi ||
+        !args->Kx || !args->Ky || !args->Kz || !args->c_r || !args->BP || !args->WP)
+        return TSE_ERR_ARG;
+    cudaStream_t stream = (cudaStream_t)stream_;
+    PressureSetup S;
+    int rc = setup_pressure(grid, args, d_ws, ws_bytes, stream, S);
+    if (rc != TSE_OK) return rc;
+    return run_dc(S, args->dt_P, args->inc_it, args->max_dt, args->min_dt, args->P_conv,
+                  args->max_it, 1, 0, cycle, args->SOR, PA_P, args->P, d_status, stream);
+}
+
+extern "C" int32_t tse_compute_C_dc(const TseGrid* grid, const TseSpeciesArgs* a, int32_t cycle,
+                                    TseSolveStatus* d_status, void* d_ws, size_t ws_bytes,
+                                    void* stream_) {
+    if (!grid || !a || !d_status || !d_ws) return TSE_ERR_ARG;
+    if (grid->nx < 1 || grid->ny < 1 || grid->nz < 1 || a->max_it < 1) return TSE_ERR_ARG;
+    if (!a->C || !a->D_fx || !a->D_fy || !a->D_fz || !a->phi || !a->rho_f || !a->qx || !a->qy ||
+        !a->qz || !a->BC || !a->WC || !a->RC || !a->e || !a->l_l || !a->l_t)
+        return TSE_ERR_ARG;
+    cudaStream_t stream = (cudaStream_t)stream_;
+    TransportSetup S;
+    int rc = setup_species(grid, a, d_ws, ws_bytes, stream, S);
+    if (rc != TSE_OK) return rc;
+    return run_dc(S, a->dt, a->inc_it, a->max_dt, a->min_dt, a->conv, a->max_it, 0,
+                  a->omega == 0.0, cycle, a->SOR, TA_X, a->C, d_status, stream);
+}
+
+extern "C" int32_t tse_compute_T_dc(const TseGrid* grid, const TseHeatArgs* a, int32_t cycle,
+                                    TseSolveStatus* d_status, void* d_ws, size_t ws_bytes,
+                                    void* stream_) {
+    if (!grid || !a || !d_status || !d_ws) return TSE_ERR_ARG;
+    if (grid->nx < 1 || grid->ny < 1 || grid->nz < 1 || a->max_it < 1) return TSE_ERR_ARG;
+    if (!a->T || !a->l_f || !a->cp_f || !a->rho_f || !a->phi || !a->qx || !a->qy || !a->qz ||
+        !a->BT || !a->WT || !a->e || !a->l_r || !a->rho_r || !a->cp_r || !a->l_l || !a->l_t)
+        return TSE_ERR_ARG;
+    cudaStream_t stream = (cudaStream_t)stream_;
+    TransportSetup S;
+    int rc = setup_heat(grid, a, d_ws, ws_bytes, stream, S);
+    if (rc != TSE_OK) return rc;
+    return run_dc(S, a->dt, a->inc_it, a->max_dt, a->min_dt, a->conv, a->max_it, 0,
+                  a->omega == 0.0, cycle, a->SOR, TA_X, a->T, d_status, stream);
+}

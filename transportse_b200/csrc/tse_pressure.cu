@@ -12,57 +12,10 @@
 // reference's.  Compiled with --fmad=false.
 #include <atomic>
 
+#include "tse_forms.cuh"
 #include "tse_rbsolve.cuh"
 
 namespace tse {
-
-enum PArr {
-    PA_A = 0, PA_C, PA_E, PA_G, PA_I, PA_K,   // transmissibilities x+ x- y+ y- z+ z-
-    PA_AB, PA_CD, PA_IJ, PA_KL,               // buoyancy products
-    PA_RPN, PA_WP, PA_DEN,                    // R*Pn, WP, R+M
-    PA_S, PA_M, PA_PN,                        // storage numerator, M, Pn (reset)
-    PA_P,                                     // solution
-    PA_COUNT
-};
-
-struct PressureForm {
-    double* arr[2];   // per colour: PA_COUNT arrays of Ncal doubles
-    long long Ncal, SX;
-    int H;
-    int xgrav, zgrav;
-    double SOR;
-
-    __device__ __forceinline__ const double* a(int col, int k) const { return arr[col] + (long long)k * Ncal; }
-
-    __device__ __forceinline__ double update(int col, long long m, uint8_t f, double xold,
-                                             const double* Xo) const {
-        const double* b = arr[col];
-        double s = (f & F_XP) ? b[PA_A * Ncal + m] * __ldcg(Xo + m + SX) : 0.0;
-        s = s + (xgrav ? b[PA_AB * Ncal + m] : 0.0);
-        s = s + ((f & F_XM) ? b[PA_C * Ncal + m] * __ldcg(Xo + m - SX) : 0.0);
-        s = s - (xgrav ? b[PA_CD * Ncal + m] : 0.0);
-        s = s + ((f & F_YP) ? b[PA_E * Ncal + m] * __ldcg(Xo + m + H) : 0.0);
-        s = s + ((f & F_YM) ? b[PA_G * Ncal + m] * __ldcg(Xo + m - H) : 0.0);
-        const long long zo = (long long)(f >> 7);
-        s = s + ((f & F_ZP) ? b[PA_I * Ncal + m] * __ldcg(Xo + m + zo) : 0.0);
-        s = s + (zgrav ? b[PA_IJ * Ncal + m] : 0.0);
-        s = s + ((f & F_ZM) ? b[PA_K * Ncal + m] * __ldcg(Xo + m - 1 + zo) : 0.0);
-        s = s - (zgrav ? b[PA_KL * Ncal + m] : 0.0);
-        s = s + b[PA_RPN * Ncal + m];
-        s = s + b[PA_WP * Ncal + m];
-        return (1.0 - SOR) * xold + (SOR * s) / b[PA_DEN * Ncal + m];
-    }
-
-    // dt halving: P = Pn (tse.py:738) and the dt-dependent R terms
-    __device__ __forceinline__ void reassemble(int col, long long m, double dt) const {
-        double* b = arr[col];
-        const double pn = b[PA_PN * Ncal + m];
-        const double R = b[PA_S * Ncal + m] / dt;
-        b[PA_RPN * Ncal + m] = R * pn;
-        b[PA_DEN * Ncal + m] = R + b[PA_M * Ncal + m];
-        b[PA_P * Ncal + m] = pn;
-    }
-};
 
 // alpha (tse.py:249-260) for the face between cells o (first) and c
 __device__ __forceinline__ double alpha_(double K1, double K2, double n1, double n2, double r1,
@@ -177,6 +130,48 @@ size_t pressure_ws_bytes(const Layout& L, long long* Ncal_out) {
     return b;
 }
 
+// Carve the workspace and launch the assembly (shared by the exact and the
+// defect-correction pressure solves).  The bytes after the exact form's
+// arrays are returned in `tail` for the caller's own use.
+int setup_pressure(const TseGrid* grid, const TsePressureArgs* args, void* d_ws, size_t ws_bytes,
+                   cudaStream_t stream, PressureSetup& S) {
+    S.L = make_layout(grid->nx, grid->ny, grid->nz);
+    const size_t need = pressure_ws_bytes(S.L, &S.Ncal);
+    if (need > ws_bytes) return TSE_ERR_WORKSPACE;
+    char* p = (char*)d_ws;
+    S.bar = (GridBarrier*)p;
+    p += align256(sizeof(GridBarrier));
+    S.partials = (double*)p;
+    p += align256((size_t)2 * kMaxBlocks * sizeof(double));
+    S.mask[0] = (uint8_t*)p;
+    p += align256((size_t)S.Ncal);
+    S.mask[1] = (uint8_t*)p;
+    p += align256((size_t)S.Ncal);
+    double* arr0 = (double*)p;
+    S.F.arr[0] = arr0;
+    S.F.arr[1] = arr0 + (size_t)PA_COUNT * S.Ncal;
+    S.F.Ncal = S.Ncal;
+    S.F.SX = S.L.SX;
+    S.F.H = S.L.H;
+    S.F.xgrav = grid->sin_beta != 0.0;
+    S.F.zgrav = grid->cos_beta != 0.0;
+    S.F.SOR = args->SOR;
+    S.tail = (char*)d_ws + need;
+    S.tail_bytes = ws_bytes - need;
+    if (cudaMemsetAsync(S.bar, 0, sizeof(GridBarrier), stream) != cudaSuccess) return TSE_ERR_LAUNCH;
+    const long long total = (long long)S.L.nx * S.L.ny * S.L.nzp;
+    assemble_p_kernel<<<(unsigned)((total + kBlock - 1) / kBlock), kBlock, 0, stream>>>(
+        *grid, *args, S.F, S.mask[0], S.mask[1], S.L);
+    return cudaGetLastError() == cudaSuccess ? TSE_OK : TSE_ERR_LAUNCH;
+}
+
+int launch_unpack(double* out, const double* X0, const double* X1, const Layout& L,
+                  cudaStream_t stream) {
+    const long long nat = (long long)L.nx * L.ny * L.nz;
+    unpack_kernel<<<(unsigned)((nat + kBlock - 1) / kBlock), kBlock, 0, stream>>>(out, X0, X1, L);
+    return cudaGetLastError() == cudaSuccess ? TSE_OK : TSE_ERR_LAUNCH;
+}
+
 }  // namespace tse
 
 using namespace tse;
@@ -191,36 +186,11 @@ extern "C" int32_t tse_compute_P(const TseGrid* grid, const TsePressureArgs* arg
         return TSE_ERR_ARG;
     if (args->max_it < 1) return TSE_ERR_ARG;
     cudaStream_t stream = (cudaStream_t)stream_;
-    Layout L = make_layout(grid->nx, grid->ny, grid->nz);
-    long long Ncal = 0;
-    if (pressure_ws_bytes(L, &Ncal) > ws_bytes) return TSE_ERR_WORKSPACE;
-    char* p = (char*)d_ws;
-    GridBarrier* bar = (GridBarrier*)p;
-    p += align256(sizeof(GridBarrier));
-    double* partials = (double*)p;
-    p += align256((size_t)2 * kMaxBlocks * sizeof(double));
-    uint8_t* mask0 = (uint8_t*)p;
-    p += align256((size_t)Ncal);
-    uint8_t* mask1 = (uint8_t*)p;
-    p += align256((size_t)Ncal);
-    double* arr0 = (double*)p;
-    double* arr1 = arr0 + (size_t)PA_COUNT * Ncal;
-
-    PressureForm F;
-    F.arr[0] = arr0;
-    F.arr[1] = arr1;
-    F.Ncal = Ncal;
-    F.SX = L.SX;
-    F.H = L.H;
-    F.xgrav = grid->sin_beta != 0.0;
-    F.zgrav = grid->cos_beta != 0.0;
-    F.SOR = args->SOR;
-
-    if (cudaMemsetAsync(bar, 0, sizeof(GridBarrier), stream) != cudaSuccess) return TSE_ERR_LAUNCH;
-    const long long total = (long long)L.nx * L.ny * L.nzp;
-    assemble_p_kernel<<<(unsigned)((total + kBlock - 1) / kBlock), kBlock, 0, stream>>>(
-        *grid, *args, F, mask0, mask1, L);
-    if (cudaGetLastError() != cudaSuccess) return TSE_ERR_LAUNCH;
+    PressureSetup S;
+    int rc = setup_pressure(grid, args, d_ws, ws_bytes, stream, S);
+    if (rc != TSE_OK) return rc;
+    const Layout L = S.L;
+    const long long Ncal = S.Ncal;
 
     SolveCtl ctl;
     ctl.L = L;
@@ -233,21 +203,16 @@ extern "C" int32_t tse_compute_P(const TseGrid* grid, const TsePressureArgs* arg
     ctl.max_it = args->max_it;
     ctl.pressure_schedule = 1;
     ctl.stop_on_first = 0;
-    ctl.X[0] = arr0 + (size_t)PA_P * Ncal;
-    ctl.X[1] = arr1 + (size_t)PA_P * Ncal;
-    ctl.mask[0] = mask0;
-    ctl.mask[1] = mask1;
-    ctl.partials = partials;
-    ctl.bar = bar;
+    ctl.X[0] = S.F.arr[0] + (size_t)PA_P * Ncal;
+    ctl.X[1] = S.F.arr[1] + (size_t)PA_P * Ncal;
+    ctl.mask[0] = S.mask[0];
+    ctl.mask[1] = S.mask[1];
+    ctl.partials = S.partials;
+    ctl.bar = S.bar;
     ctl.status = d_status;
-    int rc = launch_rb_solve(F, ctl, stream);
+    rc = launch_rb_solve(S.F, ctl, stream);
     if (rc != TSE_OK) return rc;
-
-    const long long nat = (long long)L.nx * L.ny * L.nz;
-    unpack_kernel<<<(unsigned)((nat + kBlock - 1) / kBlock), kBlock, 0, stream>>>(
-        args->P, ctl.X[0], ctl.X[1], L);
-    if (cudaGetLastError() != cudaSuccess) return TSE_ERR_LAUNCH;
-    return TSE_OK;
+    return launch_unpack(args->P, ctl.X[0], ctl.X[1], L, stream);
 }
 
 // ----------------------------------------------------------------------------

@@ -132,6 +132,7 @@ __global__ void __launch_bounds__(kBlock, 3) rb_solve_kernel(Form F, SolveCtl c)
         s->halvings = halvings;
         s->error = err ? TSE_STATUS_BARRIER_TIMEOUT : TSE_STATUS_OK;
         s->n_events = nev < 8 ? nev : 8;
+        s->cycles = 0;
     }
 }
 

@@ -9,54 +9,10 @@
 //   X = (1-SOR) X + SOR (omega (Mnew+Nnew+Onew+Pnew+Qnew+Rnew)
 //                        + (1-omega) (...) + R Xn + W - E) / (R - omega M)
 // (tse.py:870-875, 1038-1043) term by term.  Compiled with --fmad=false.
+#include "tse_forms.cuh"
 #include "tse_rbsolve.cuh"
 
 namespace tse {
-
-enum TArr {
-    TA_A = 0, TA_B, TA_C, TA_D, TA_E, TA_F,   // neighbour coefficients x+ x- y+ y- z+ z-
-    TA_Y,                                     // (1-omega) * (Xn M + old neighbour sum)
-    TA_RXN, TA_W, TA_EX, TA_DEN,              // R Xn, source, IMBLFLO term, R - omega M
-    TA_RNUM, TA_M, TA_XN,                     // R numerator, M, Xn (reset)
-    TA_X,                                     // solution
-    TA_COUNT
-};
-
-struct TransportForm {
-    double* arr[2];
-    long long Ncal, SX;
-    int H;
-    int useY, useEX;
-    double omega, SOR;
-
-    __device__ __forceinline__ double update(int col, long long m, uint8_t f, double xold,
-                                             const double* Xo) const {
-        const double* b = arr[col];
-        const long long zo = (long long)(f >> 7);
-        double s = (f & F_XP) ? b[TA_A * Ncal + m] * __ldcg(Xo + m + SX) : 0.0;
-        s = s + ((f & F_XM) ? b[TA_B * Ncal + m] * __ldcg(Xo + m - SX) : 0.0);
-        s = s + ((f & F_YP) ? b[TA_C * Ncal + m] * __ldcg(Xo + m + H) : 0.0);
-        s = s + ((f & F_YM) ? b[TA_D * Ncal + m] * __ldcg(Xo + m - H) : 0.0);
-        s = s + ((f & F_ZP) ? b[TA_E * Ncal + m] * __ldcg(Xo + m + zo) : 0.0);
-        s = s + ((f & F_ZM) ? b[TA_F * Ncal + m] * __ldcg(Xo + m - 1 + zo) : 0.0);
-        double num = omega * s;
-        if (useY) num = num + b[TA_Y * Ncal + m];
-        num = num + b[TA_RXN * Ncal + m];
-        num = num + b[TA_W * Ncal + m];
-        num = num - (useEX ? b[TA_EX * Ncal + m] : 0.0);
-        return (1.0 - SOR) * xold + (SOR * num) / b[TA_DEN * Ncal + m];
-    }
-
-    // dt halving: X = Xn (tse.py:911, 1077) and the dt-dependent R terms
-    __device__ __forceinline__ void reassemble(int col, long long m, double dt) const {
-        double* b = arr[col];
-        const double xn = b[TA_XN * Ncal + m];
-        const double R = b[TA_RNUM * Ncal + m] / dt;
-        b[TA_RXN * Ncal + m] = R * xn;
-        b[TA_DEN * Ncal + m] = R - omega * b[TA_M * Ncal + m];
-        b[TA_X * Ncal + m] = xn;
-    }
-};
 
 // dispersivity (tse.py:460-644); D = {xl, yl, zl, xr, yr, zr}
 __device__ void dispersivity_dev(const double* qx, const double* qy, const double* qz,
@@ -408,53 +364,67 @@ size_t transport_ws_bytes(const Layout& L, long long* Ncal_out) {
     return b;
 }
 
-struct TransportWs {
-    GridBarrier* bar;
-    double* partials;
-    uint8_t* mask[2];
-    double* arr[2];
-    long long Ncal;
-};
-
-static int carve_transport(const Layout& L, void* ws, size_t bytes, TransportWs& w) {
-    if (transport_ws_bytes(L, &w.Ncal) > bytes) return TSE_ERR_WORKSPACE;
-    char* p = (char*)ws;
-    w.bar = (GridBarrier*)p;
+// Carve the workspace and launch the assembly (shared by the exact and the
+// defect-correction transport solves).
+template <class Args, class AssembleK>
+static int setup_transport(const TseGrid* grid, const Args* a, void* d_ws, size_t ws_bytes,
+                           cudaStream_t stream, AssembleK kernel, int imbl, TransportSetup& S) {
+    S.L = make_layout(grid->nx, grid->ny, grid->nz);
+    const size_t need = transport_ws_bytes(S.L, &S.Ncal);
+    if (need > ws_bytes) return TSE_ERR_WORKSPACE;
+    char* p = (char*)d_ws;
+    S.bar = (GridBarrier*)p;
     p += align256(sizeof(GridBarrier));
-    w.partials = (double*)p;
+    S.partials = (double*)p;
     p += align256((size_t)2 * kMaxBlocks * sizeof(double));
-    w.mask[0] = (uint8_t*)p;
-    p += align256((size_t)w.Ncal);
-    w.mask[1] = (uint8_t*)p;
-    p += align256((size_t)w.Ncal);
-    w.arr[0] = (double*)p;
-    w.arr[1] = w.arr[0] + (size_t)TA_COUNT * w.Ncal;
-    return TSE_OK;
+    S.mask[0] = (uint8_t*)p;
+    p += align256((size_t)S.Ncal);
+    S.mask[1] = (uint8_t*)p;
+    p += align256((size_t)S.Ncal);
+    S.F.arr[0] = (double*)p;
+    S.F.arr[1] = S.F.arr[0] + (size_t)TA_COUNT * S.Ncal;
+    S.F.Ncal = S.Ncal;
+    S.F.SX = S.L.SX;
+    S.F.H = S.L.H;
+    S.F.omega = a->omega;
+    S.F.SOR = a->SOR;
+    S.F.useY = a->omega != 1.0;
+    S.F.useEX = imbl != 0;
+    S.tail = (char*)d_ws + need;
+    S.tail_bytes = ws_bytes - need;
+    if (cudaMemsetAsync(S.bar, 0, sizeof(GridBarrier), stream) != cudaSuccess) return TSE_ERR_LAUNCH;
+    const long long total = (long long)S.L.nx * S.L.ny * S.L.nzp;
+    kernel<<<(unsigned)((total + kBlock - 1) / kBlock), kBlock, 0, stream>>>(*grid, *a, S.F, S.mask[0],
+                                                                              S.mask[1], S.L);
+    return cudaGetLastError() == cudaSuccess ? TSE_OK : TSE_ERR_LAUNCH;
+}
+
+int setup_species(const TseGrid* grid, const TseSpeciesArgs* a, void* d_ws, size_t ws_bytes,
+                  cudaStream_t stream, TransportSetup& S) {
+    return setup_transport(grid, a, d_ws, ws_bytes, stream, assemble_c_kernel, a->imblflo, S);
+}
+
+int setup_heat(const TseGrid* grid, const TseHeatArgs* a, void* d_ws, size_t ws_bytes,
+               cudaStream_t stream, TransportSetup& S) {
+    return setup_transport(grid, a, d_ws, ws_bytes, stream, assemble_t_kernel, a->imblflo, S);
 }
 
 template <class Args, class AssembleK>
 static int run_transport(const TseGrid* grid, const Args* a, double* X, TseSolveStatus* d_status,
                          void* d_ws, size_t ws_bytes, void* stream_, AssembleK kernel, int imbl) {
     cudaStream_t stream = (cudaStream_t)stream_;
-    Layout L = make_layout(grid->nx, grid->ny, grid->nz);
-    TransportWs w;
-    int rc = carve_transport(L, d_ws, ws_bytes, w);
+    TransportSetup S;
+    int rc = setup_transport(grid, a, d_ws, ws_bytes, stream, kernel, imbl, S);
     if (rc != TSE_OK) return rc;
-    TransportForm F;
-    F.arr[0] = w.arr[0];
-    F.arr[1] = w.arr[1];
-    F.Ncal = w.Ncal;
-    F.SX = L.SX;
-    F.H = L.H;
-    F.omega = a->omega;
-    F.SOR = a->SOR;
-    F.useY = a->omega != 1.0;
-    F.useEX = imbl != 0;
-    if (cudaMemsetAsync(w.bar, 0, sizeof(GridBarrier), stream) != cudaSuccess) return TSE_ERR_LAUNCH;
-    const long long total = (long long)L.nx * L.ny * L.nzp;
-    kernel<<<(unsigned)((total + kBlock - 1) / kBlock), kBlock, 0, stream>>>(*grid, *a, F, w.mask[0],
-                                                                              w.mask[1], L);
-    if (cudaGetLastError() != cudaSuccess) return TSE_ERR_LAUNCH;
+    const Layout L = S.L;
+    TransportForm F = S.F;
+    struct {
+        GridBarrier* bar;
+        double* partials;
+        uint8_t* mask[2];
+        double* arr[2];
+        long long Ncal;
+    } w = {S.bar, S.partials, {S.mask[0], S.mask[1]}, {S.F.arr[0], S.F.arr[1]}, S.Ncal};
     SolveCtl ctl;
     ctl.L = L;
     ctl.Ncal = w.Ncal;

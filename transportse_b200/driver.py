@@ -50,7 +50,10 @@ def pymin(*a):
 
 
 class Simulation:
-    def __init__(self, config, device=None, verbose=False):
+    def __init__(self, config, device=None, verbose=False, precision=None):
+        """precision: 'fp64' (the reference's arithmetic) or 'fp32dc' (FP32
+        sweeps with FP64 defect correction); default: config.GPU_PRECISION,
+        else 'fp64'."""
         if config.CHEMREACT:
             raise NotImplementedError("CHEMREACT: chemistry coupling is not part of the GPU "
                                       "time-step core")
@@ -59,7 +62,7 @@ class Simulation:
         self.config = config
         self.verbose = verbose
         self.device = torch.device(device if device is not None else "cuda")
-        self.M = Model.from_config(config, device=self.device)
+        self.M = Model.from_config(config, device=self.device, precision=precision)
         self.shape = (int(config.nx), int(config.ny), int(config.nz))
         self.S = {}
         self.upload_state(config)

@@ -32,7 +32,17 @@ def _sin_cos_beta(beta_deg):
 
 
 class Model:
-    def __init__(self, nx, ny, nz, dx, dy, dz, g, beta_deg, device=None):
+    PRECISIONS = ("fp64", "fp32dc")
+
+    def __init__(self, nx, ny, nz, dx, dy, dz, g, beta_deg, device=None, precision="fp64",
+                 dc_cycle=128):
+        """precision 'fp64': the reference's arithmetic, operation for
+        operation; 'fp32dc': FP32 sweeps on a correction driven by an FP64
+        residual (tse_compute_*_dc), same convergence test and dt control."""
+        if precision not in self.PRECISIONS:
+            raise ValueError("precision must be one of %s" % (self.PRECISIONS,))
+        self.precision = precision
+        self.dc_cycle = int(dc_cycle)
         self.device = torch.device(device if device is not None else "cuda")
         if self.device.type != "cuda":
             raise RuntimeError("transportse_b200 kernels run on CUDA devices only")
@@ -49,9 +59,10 @@ class Model:
                               self.cosb)
         L = N.lib()
         gp = ct.byref(self.grid)
-        self.ws_bytes = max(L.tse_workspace_bytes(gp, N.TSE_WS_PRESSURE),
-                            L.tse_workspace_bytes(gp, N.TSE_WS_TRANSPORT),
-                            L.tse_workspace_bytes(gp, N.TSE_WS_REDUCE))
+        kinds = (N.TSE_WS_PRESSURE, N.TSE_WS_TRANSPORT, N.TSE_WS_REDUCE)
+        if precision == "fp32dc":
+            kinds += (N.TSE_WS_PRESSURE_DC, N.TSE_WS_TRANSPORT_DC)
+        self.ws_bytes = max(L.tse_workspace_bytes(gp, k) for k in kinds)
         self.ws = torch.empty(self.ws_bytes, dtype=torch.uint8, device=self.device)
         self.red_ws = torch.empty(L.tse_workspace_bytes(gp, N.TSE_WS_REDUCE), dtype=torch.uint8,
                                   device=self.device)
@@ -71,9 +82,29 @@ class Model:
         self.cell_updates = {"P": 0, "C": 0, "T": 0}
 
     @classmethod
-    def from_config(cls, config, device=None):
+    def from_config(cls, config, device=None, precision=None):
+        if precision is None:
+            precision = getattr(config, "GPU_PRECISION", "fp64")
         return cls(config.nx, config.ny, config.nz, config.dx, config.dy, config.dz, config.g,
-                   config.beta, device=device)
+                   config.beta, device=device, precision=precision,
+                   dc_cycle=getattr(config, "GPU_DC_CYCLE", 128))
+
+    # FP32 corrections resolve a relative change of about 1e-13 of the FP64
+    # iterate at best; a solve asking for a tighter tolerance runs in FP64
+    DC_MIN_CONV = 1e-13
+
+    def _solve(self, name, args_struct, conv):
+        """Call tse_<name> or its mixed-precision form tse_<name>_dc."""
+        L = N.lib()
+        if self.precision == "fp32dc" and conv >= getattr(self, "dc_min_conv", self.DC_MIN_CONV):
+            rc = getattr(L, "tse_%s_dc" % name)(ct.byref(self.grid), ct.byref(args_struct),
+                                                self.dc_cycle, self._p(self.status),
+                                                self._p(self.ws), self.ws_bytes, self._stream())
+        else:
+            rc = getattr(L, "tse_" + name)(ct.byref(self.grid), ct.byref(args_struct),
+                                           self._p(self.status), self._p(self.ws), self.ws_bytes,
+                                           self._stream())
+        N.check(rc, "tse_" + name)
 
     # ----------------------------------------------------------- helpers
     def _t(self, a):
@@ -149,9 +180,7 @@ class Model:
             float(dt_P), float(SOR), float(inc_it), float(max_dt), float(min_dt), float(P_conv))
         a.max_it = int(max_it)
         ev = self._ev_start()
-        rc = N.lib().tse_compute_P(ct.byref(self.grid), ct.byref(a), self._p(self.status),
-                                   self._p(self.ws), self.ws_bytes, self._stream())
-        N.check(rc, "tse_compute_P")
+        self._solve("compute_P", a, a.P_conv)
         self.launches += 3
         ev = self._ev_end(ev)
         s = self.read_status()
@@ -199,9 +228,7 @@ class Model:
         a.max_it = int(max_it)
         a.imblflo = int(self.C_IMBLFLO)
         ev = self._ev_start()
-        rc = N.lib().tse_compute_C(ct.byref(self.grid), ct.byref(a), self._p(self.status),
-                                   self._p(self.ws), self.ws_bytes, self._stream())
-        N.check(rc, "tse_compute_C")
+        self._solve("compute_C", a, a.conv)
         self.launches += 3
         ev = self._ev_end(ev)
         s = self.read_status()
@@ -228,9 +255,7 @@ class Model:
         a.max_it = int(max_it)
         a.imblflo = int(self.T_IMBLFLO)
         ev = self._ev_start()
-        rc = N.lib().tse_compute_T(ct.byref(self.grid), ct.byref(a), self._p(self.status),
-                                   self._p(self.ws), self.ws_bytes, self._stream())
-        N.check(rc, "tse_compute_T")
+        self._solve("compute_T", a, a.conv)
         self.launches += 3
         ev = self._ev_end(ev)
         s = self.read_status()
