@@ -132,20 +132,27 @@ int32_t tse_compute_P(const TseGrid *grid, const TsePressureArgs *args,
 /* Mixed-precision forms of compute_P / compute_C / compute_T (tse.py:647,
  * 783, 919): the FP64 residual of the reference's per-cell equation drives
  * red-black SOR sweeps on an FP32 correction, which is added to the FP64
- * iterate every `cycle` iterations (<= 0: 128) and at convergence.  Same
- * arguments, convergence test, dt control and results as the FP64 entry
- * points; agreement with them is to the solver tolerance, not bit for bit.
+ * iterate every `cycle` iterations and at convergence.  Same arguments,
+ * convergence test, dt control and results as the FP64 entry points;
+ * agreement with them is to the solver tolerance, not bit for bit.  These
+ * calls synchronise the stream once per correction cycle (they read the
+ * sweep kernel's event record) and return when the solve is done.
  * Workspace: TSE_WS_PRESSURE_DC / TSE_WS_TRANSPORT_DC. */
+typedef struct TseDcOptions {
+    int32_t cycle;       /* iterations per correction cycle, <= 0: 128 */
+    int32_t max_blocks;  /* cap on the sweep kernel's blocks, <= 0: as many as
+                            fit; lets several solves share the GPU at once */
+} TseDcOptions;
 int32_t tse_compute_P_dc(const TseGrid *grid, const TsePressureArgs *args,
-                         int32_t cycle, TseSolveStatus *d_status,
+                         const TseDcOptions *opts, TseSolveStatus *d_status,
                          void *d_workspace, size_t workspace_bytes,
                          void *stream);
 int32_t tse_compute_C_dc(const TseGrid *grid, const TseSpeciesArgs *args,
-                         int32_t cycle, TseSolveStatus *d_status,
+                         const TseDcOptions *opts, TseSolveStatus *d_status,
                          void *d_workspace, size_t workspace_bytes,
                          void *stream);
 int32_t tse_compute_T_dc(const TseGrid *grid, const TseHeatArgs *args,
-                         int32_t cycle, TseSolveStatus *d_status,
+                         const TseDcOptions *opts, TseSolveStatus *d_status,
                          void *d_workspace, size_t workspace_bytes,
                          void *stream);
 

@@ -46,7 +46,7 @@ def test_workspace_sizes_without_gpu():
 STRUCTS = {
     "TseGrid": N.TseGrid, "TseSolveStatus": N.TseSolveStatus,
     "TsePressureArgs": N.TsePressureArgs, "TseSpeciesArgs": N.TseSpeciesArgs,
-    "TseHeatArgs": N.TseHeatArgs,
+    "TseHeatArgs": N.TseHeatArgs, "TseDcOptions": N.TseDcOptions,
 }
 
 

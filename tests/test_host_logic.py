@@ -1,0 +1,110 @@
+"""Host-side logic that needs no GPU: the colour-split index arithmetic the
+kernels use, the EOS declaration check, the HBM admission budget, trace and
+workload determinism, and ensemble sharding across ranks."""
+import threading
+import time
+
+import numpy
+import pytest
+
+from transportse_b200 import eos, workloads
+
+
+def _layout(nx, ny, nz):
+    nzp = nz + (nz & 1)
+    H = nzp // 2
+    return nzp, H, ny * H
+
+
+@pytest.mark.parametrize("shape", [(3, 4, 5), (2, 1, 7), (4, 3, 6), (1, 1, 9), (5, 5, 1)])
+def test_colour_split_neighbour_arithmetic(shape):
+    """Compact index m = ((i*ny + j)*nzp + k) >> 1 per colour; neighbours of
+    the other colour at m +- SX, m +- H, m + (k&1), m - 1 + (k&1) (the
+    offsets used by the sweep kernels) -- checked against the grid."""
+    nx, ny, nz = shape
+    nzp, H, SX = _layout(nx, ny, nz)
+    idx = {}
+    for i in range(nx):
+        for j in range(ny):
+            for k in range(nzp):
+                col = (i + j + k) & 1
+                m = ((i * ny + j) * nzp + k) >> 1
+                assert (col, m) not in idx
+                idx[(col, m)] = (i, j, k)
+    assert len(idx) == 2 * nx * ny * H
+    for (col, m), (i, j, k) in idx.items():
+        if k >= nz:
+            continue
+        other = 1 - col
+        # the reference's red cells: (i + j + k) % 2 == 0 (tse.py:170-176)
+        assert (col == 0) == ((i + j + k) % 2 == 0)
+        if i < nx - 1:
+            assert idx[(other, m + SX)] == (i + 1, j, k)
+        if i > 0:
+            assert idx[(other, m - SX)] == (i - 1, j, k)
+        if j < ny - 1:
+            assert idx[(other, m + H)] == (i, j + 1, k)
+        if j > 0:
+            assert idx[(other, m - H)] == (i, j - 1, k)
+        if k < nz - 1:
+            assert idx[(other, m + (k & 1))] == (i, j, k + 1)
+        if k > 0:
+            assert idx[(other, m - 1 + (k & 1))] == (i, j, k - 1)
+
+
+def test_declared_eos_validates_against_callback():
+    cfg = workloads.reservoir_3d(6, 5, 4, seed=1)
+    decl = eos.declared_eos(cfg)
+    assert eos.validate(cfg, decl)
+    bad = dict(decl)
+    bad["rho"] = dict(decl["rho"], tcoef=0.31)
+    with pytest.raises(eos.EOSMismatch):
+        eos.validate(cfg, bad)
+
+
+def test_hbm_budget_blocks_until_release():
+    from transportse_b200.ensemble import HbmBudget
+    b = HbmBudget(100)
+    assert b.acquire(60)
+    got = []
+
+    def late():
+        got.append(b.acquire(50))
+
+    th = threading.Thread(target=late)
+    th.start()
+    time.sleep(0.2)
+    assert not got            # 60 + 50 > 100: waits
+    b.release(60)
+    th.join(timeout=5)
+    assert got == [True]
+    with pytest.raises(MemoryError):
+        b.acquire(101)
+
+
+def test_poisson_trace_is_seeded():
+    from transportse_b200.serving import poisson_trace
+    a = poisson_trace(5, 20.0, 3, workloads.serving_request, 2, n_min=8, n_max=12)
+    b = poisson_trace(5, 20.0, 3, workloads.serving_request, 2, n_min=8, n_max=12)
+    assert [x[0] for x in a] == [x[0] for x in b]
+    assert a[0][0] == 0.0 and all(a[i][0] <= a[i + 1][0] for i in range(4))
+    assert [x[1].nx for x in a] == [x[1].nx for x in b]
+
+
+def test_workload_builders_are_deterministic():
+    from tests.golden.cases import config_checksum
+    for f, kw in ((workloads.reservoir_3d, dict(nx=8, ny=6, nz=5, seed=4)),
+                  (workloads.sloped_3d, dict(nx=6, ny=5, nz=4, seed=2)),
+                  (workloads.ensemble_member, dict(seed=7)),
+                  (workloads.serving_request, dict(seed=8, n=10))):
+        assert config_checksum(f(**kw)) == config_checksum(f(**kw))
+
+
+def test_shard_balances_and_covers():
+    from transportse_b200.ensemble import shard
+    sizes = [int(x) for x in numpy.random.default_rng(0).integers(1000, 100000, 37)]
+    parts = [shard(sizes, r, 4) for r in range(4)]
+    flat = sorted(i for p in parts for i in p)
+    assert flat == list(range(37))
+    loads = [sum(sizes[i] for i in p) for p in parts]
+    assert max(loads) <= 1.25 * (sum(sizes) / 4) + max(sizes)

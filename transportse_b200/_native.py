@@ -64,6 +64,10 @@ class TseHeatArgs(ct.Structure):
         [("max_it", ct.c_int32), ("imblflo", ct.c_int32)]
 
 
+class TseDcOptions(ct.Structure):
+    _fields_ = [("cycle", ct.c_int32), ("max_blocks", ct.c_int32)]
+
+
 # name -> (restype, argtypes)
 _P = ct.c_void_p
 _I = ct.c_int32
@@ -75,9 +79,12 @@ SIGNATURES = {
     "tse_workspace_bytes": (ct.c_size_t, [_G, _I]),
     "tse_compute_P": (_I, [_G, ct.POINTER(TsePressureArgs), _P, _P, _S, _P]),
     "tse_compute_P_noalloc": (_I, [_G, ct.POINTER(TsePressureArgs), _P, _P]),
-    "tse_compute_P_dc": (_I, [_G, ct.POINTER(TsePressureArgs), _I, _P, _P, _S, _P]),
-    "tse_compute_C_dc": (_I, [_G, ct.POINTER(TseSpeciesArgs), _I, _P, _P, _S, _P]),
-    "tse_compute_T_dc": (_I, [_G, ct.POINTER(TseHeatArgs), _I, _P, _P, _S, _P]),
+    "tse_compute_P_dc": (_I, [_G, ct.POINTER(TsePressureArgs), ct.POINTER(TseDcOptions), _P, _P,
+                              _S, _P]),
+    "tse_compute_C_dc": (_I, [_G, ct.POINTER(TseSpeciesArgs), ct.POINTER(TseDcOptions), _P, _P,
+                              _S, _P]),
+    "tse_compute_T_dc": (_I, [_G, ct.POINTER(TseHeatArgs), ct.POINTER(TseDcOptions), _P, _P, _S,
+                              _P]),
     "tse_compute_q": (_I, [_G, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "tse_flow_error": (_I, [_G, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _D, _P, _P]),
     "tse_compute_C": (_I, [_G, ct.POINTER(TseSpeciesArgs), _P, _P, _S, _P]),

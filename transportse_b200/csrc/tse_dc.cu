@@ -17,8 +17,8 @@
 // d's rounding and the iteration counts track the FP64 form's.
 //
 // Kernels: the FP32 sweeps run in one cooperative kernel that iterates until
-// an event (converged, cycle end, dt halving, stop); it needs ~40 registers,
-// so 6 blocks fit per SM.  The FP64 residual, the x += d update and the dt
+// an event (converged, cycle end, dt halving, stop); it needs 48 registers,
+// so 5 blocks fit per SM.  The FP64 residual, the x += d update and the dt
 // halving (reset + new R terms) are separate, ordinary kernels, so their
 // register appetite does not limit the sweeps' occupancy.  The host reads one
 // small state record per correction cycle.
@@ -352,7 +352,7 @@ size_t dc_extra_bytes(const Layout& L) {
            align256(sizeof(DcState)) + 512;
 }
 
-static int sweep_blocks(long long Nc) {
+static int sweep_blocks(long long Nc, int cap) {
     static int cached_dev = -1, cached_per_sm = 0, cached_sms = 0;
     int dev = 0;
     cudaGetDevice(&dev);
@@ -367,14 +367,17 @@ static int sweep_blocks(long long Nc) {
     long long nb = want < maxb ? want : maxb;
     // the setup's partials region holds 2 * kMaxBlocks doubles
     if (nb > kMaxBlocks / 2) nb = kMaxBlocks / 2;
+    if (cap > 0 && nb > cap) nb = cap;
     return (int)nb;
 }
 
 template <class Form>
 static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, double min_dt,
-                  double conv, int max_it, int pressure_schedule, int stop_on_first, int cycle,
-                  double sor, int x_index, double* X_out, TseSolveStatus* d_status,
-                  cudaStream_t stream) {
+                  double conv, int max_it, int pressure_schedule, int stop_on_first,
+                  const TseDcOptions* opts, double sor, int x_index, double* X_out,
+                  TseSolveStatus* d_status, cudaStream_t stream) {
+    const int cycle = opts ? opts->cycle : 0;
+    const int cap = opts ? opts->max_blocks : 0;
     if (S.tail_bytes < dc_extra_bytes(S.L)) return TSE_ERR_WORKSPACE;
     DcCtl c;
     c.L = S.L;
@@ -412,7 +415,7 @@ static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, 
         return TSE_ERR_LAUNCH;
     const long long cells2 = 2 * S.L.Nc;
     const unsigned gcells = (unsigned)((cells2 + kBlock - 1) / kBlock);
-    const int nb = sweep_blocks(S.L.Nc);
+    const int nb = sweep_blocks(S.L.Nc, cap);
     dc_scale_kernel<<<gcells, kBlock, 0, stream>>>(S.F, c);
     if (cudaGetLastError() != cudaSuccess) return TSE_ERR_LAUNCH;
     for (;;) {
@@ -449,7 +452,8 @@ static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, 
 
 using namespace tse;
 
-extern "C" int32_t tse_compute_P_dc(const TseGrid* grid, const TsePressureArgs* args, int32_t cycle,
+extern "C" int32_t tse_compute_P_dc(const TseGrid* grid, const TsePressureArgs* args,
+                                    const TseDcOptions* opts,
                                     TseSolveStatus* d_status, void* d_ws, size_t ws_bytes,
                                     void* stream_) {
     if (!grid || !args || !d_status || !d_ws) return TSE_ERR_ARG;
@@ -462,10 +466,11 @@ extern "C" int32_t tse_compute_P_dc(const TseGrid* grid, const TsePressureArgs* 
     int rc = setup_pressure(grid, args, d_ws, ws_bytes, stream, S);
     if (rc != TSE_OK) return rc;
     return run_dc(S, args->dt_P, args->inc_it, args->max_dt, args->min_dt, args->P_conv,
-                  args->max_it, 1, 0, cycle, args->SOR, PA_P, args->P, d_status, stream);
+                  args->max_it, 1, 0, opts, args->SOR, PA_P, args->P, d_status, stream);
 }
 
-extern "C" int32_t tse_compute_C_dc(const TseGrid* grid, const TseSpeciesArgs* a, int32_t cycle,
+extern "C" int32_t tse_compute_C_dc(const TseGrid* grid, const TseSpeciesArgs* a,
+                                    const TseDcOptions* opts,
                                     TseSolveStatus* d_status, void* d_ws, size_t ws_bytes,
                                     void* stream_) {
     if (!grid || !a || !d_status || !d_ws) return TSE_ERR_ARG;
@@ -478,10 +483,11 @@ extern "C" int32_t tse_compute_C_dc(const TseGrid* grid, const TseSpeciesArgs* a
     int rc = setup_species(grid, a, d_ws, ws_bytes, stream, S);
     if (rc != TSE_OK) return rc;
     return run_dc(S, a->dt, a->inc_it, a->max_dt, a->min_dt, a->conv, a->max_it, 0,
-                  a->omega == 0.0, cycle, a->SOR, TA_X, a->C, d_status, stream);
+                  a->omega == 0.0, opts, a->SOR, TA_X, a->C, d_status, stream);
 }
 
-extern "C" int32_t tse_compute_T_dc(const TseGrid* grid, const TseHeatArgs* a, int32_t cycle,
+extern "C" int32_t tse_compute_T_dc(const TseGrid* grid, const TseHeatArgs* a,
+                                    const TseDcOptions* opts,
                                     TseSolveStatus* d_status, void* d_ws, size_t ws_bytes,
                                     void* stream_) {
     if (!grid || !a || !d_status || !d_ws) return TSE_ERR_ARG;
@@ -494,5 +500,5 @@ extern "C" int32_t tse_compute_T_dc(const TseGrid* grid, const TseHeatArgs* a, i
     int rc = setup_heat(grid, a, d_ws, ws_bytes, stream, S);
     if (rc != TSE_OK) return rc;
     return run_dc(S, a->dt, a->inc_it, a->max_dt, a->min_dt, a->conv, a->max_it, 0,
-                  a->omega == 0.0, cycle, a->SOR, TA_X, a->T, d_status, stream);
+                  a->omega == 0.0, opts, a->SOR, TA_X, a->T, d_status, stream);
 }

@@ -1,0 +1,194 @@
+"""Ensembles of independent TRANSPORTSE models on one GPU.
+
+A parameter or permeability ensemble is a list of config modules of uneven
+grid sizes that share nothing.  ``Ensemble`` advances them concurrently: up
+to ``concurrency`` models are resident at once, each driven by its own host
+thread on its own CUDA stream through the full time-step driver
+(``driver.Simulation``: SIA loop, pressure, fluxes, transport, EOS).  The
+cooperative sweep kernels of the concurrent solves share the SMs, each capped
+to its share of the co-resident blocks, so small models fill the GPU together
+instead of each paying a whole-GPU barrier per half-sweep.  Models are
+admitted as earlier ones finish and their device memory is returned, under an
+HBM budget.
+
+The ctypes entry points release the GIL while they run, so the host threads
+overlap; every model's result is independent of which others run beside it
+(see tests/test_gpu_ensemble.py).
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import queue
+import threading
+import time
+
+import numpy
+import torch
+
+from . import _native as N
+from .driver import Simulation
+
+# resident cooperative blocks per SM of the mixed-precision sweep kernel
+SWEEP_BLOCKS_PER_SM = 5
+
+
+def state_bytes(config, precision="fp32dc"):
+    """Device bytes a resident model needs: its fields plus solver workspace."""
+    nx, ny, nz = int(config.nx), int(config.ny), int(config.nz)
+    n = nx * ny * nz
+    S = int(numpy.asarray(config.C).shape[-1])
+    nT = 2 if numpy.asarray(config.T).ndim == 4 else 1
+    # 28 3-D fields, 5 species fields, T, vx vy vz e, ZEROS ONES, Pn, rhof_prev,
+    # Cn and Tn copies
+    words = n * (28 + 5 * S + nT + 4 + 2 + 2 + S + nT)
+    g = N.TseGrid(nx, ny, nz, 0, None, None, None, 9.81, 0.0, 1.0)
+    L = N.lib()
+    kinds = [N.TSE_WS_PRESSURE, N.TSE_WS_TRANSPORT]
+    if precision == "fp32dc":
+        kinds += [N.TSE_WS_PRESSURE_DC, N.TSE_WS_TRANSPORT_DC]
+    ws = max(L.tse_workspace_bytes(ct.byref(g), k) for k in kinds)
+    return 8 * words + ws + (1 << 20)
+
+
+def shard(sizes, rank, world):
+    """Indices of the models rank ``rank`` of ``world`` runs: models are
+    independent, so ranks split them with no collective; largest first onto
+    the least loaded rank (ties to the lower rank), deterministic."""
+    order = sorted(range(len(sizes)), key=lambda i: (-sizes[i], i))
+    load = [0] * world
+    mine = []
+    for i in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        load[r] += sizes[i]
+        if r == rank:
+            mine.append(i)
+    return sorted(mine)
+
+
+def cell_updates(sim):
+    return sum(sim.M.cell_updates.values())
+
+
+class HbmBudget:
+    """Blocking byte budget for admitting models."""
+
+    def __init__(self, total_bytes):
+        self.total = int(total_bytes)
+        self.free = int(total_bytes)
+        self.cv = threading.Condition()
+
+    def acquire(self, nbytes, stop=None):
+        nbytes = int(nbytes)
+        if nbytes > self.total:
+            raise MemoryError("model needs %.2f GB, budget is %.2f GB" % (nbytes / 1e9, self.total / 1e9))
+        with self.cv:
+            while self.free < nbytes:
+                if stop is not None and stop.is_set():
+                    return False
+                self.cv.wait(timeout=0.1)
+            self.free -= nbytes
+            return True
+
+    def release(self, nbytes):
+        with self.cv:
+            self.free += int(nbytes)
+            self.cv.notify_all()
+
+
+def default_budget(device):
+    free, total = torch.cuda.mem_get_info(device)
+    return int(free * 0.85)
+
+
+def block_cap(device, concurrency):
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    return max(8, (sms * SWEEP_BLOCKS_PER_SM) // max(1, concurrency))
+
+
+def run_model(config, steps, device, precision, max_blocks, dc_cycle=None, keep=("P", "C", "T")):
+    """Run one model on the calling thread's current stream; returns results."""
+    sim = Simulation(config, device=device, precision=precision)
+    sim.M.max_blocks = int(max_blocks)
+    if dc_cycle:
+        sim.M.dc_cycle = int(dc_cycle)
+    sim.run(max_steps=steps)
+    out = {k: sim.field(k) for k in keep}
+    out["cell_updates"] = cell_updates(sim)
+    out["steps"] = sim.n_tsteps
+    out["t_sim"] = sim.t_sim
+    out["iterations"] = dict(sim.counters)
+    return out
+
+
+def autotune(configs, device=None, precision="fp32dc", steps=1,
+             concurrency=(2, 4, 8), cycles=(64, 128, 256)):
+    """Pick the concurrency (models in flight, hence blocks per model) and the
+    correction-cycle length that give the highest cell-update rate on a
+    sample of the ensemble.  Returns {"concurrency", "dc_cycle", "rate",
+    "trials"}; the sample runs from the models' initial state each time."""
+    trials = []
+    best = None
+    for k in concurrency:
+        for cyc in cycles:
+            _, st = Ensemble(configs, device=device, precision=precision, concurrency=k,
+                             dc_cycle=cyc).run(steps, keep=())
+            trials.append({"concurrency": k, "dc_cycle": cyc, "rate": st["cell_updates_per_s"]})
+            if best is None or st["cell_updates_per_s"] > best["rate"]:
+                best = dict(trials[-1])
+    best["trials"] = trials
+    return best
+
+
+class Ensemble:
+    def __init__(self, configs, device=None, precision="fp32dc", concurrency=4, hbm_budget=None,
+                 max_blocks=None, dc_cycle=None):
+        self.configs = list(configs)
+        self.device = torch.device(device if device is not None else "cuda")
+        self.precision = precision
+        self.concurrency = max(1, int(concurrency))
+        self.budget = HbmBudget(hbm_budget if hbm_budget is not None else default_budget(self.device))
+        self.max_blocks = max_blocks if max_blocks else block_cap(self.device, self.concurrency)
+        self.dc_cycle = dc_cycle
+
+    def run(self, steps, keep=("P", "C", "T")):
+        """Advance every model by ``steps`` time steps; returns (results, stats)."""
+        todo = queue.Queue()
+        for i, cfg in enumerate(self.configs):
+            todo.put((i, cfg))
+        results = [None] * len(self.configs)
+        errors = []
+        t0 = time.perf_counter()
+
+        def worker():
+            stream = torch.cuda.Stream(device=self.device)
+            while True:
+                try:
+                    i, cfg = todo.get_nowait()
+                except queue.Empty:
+                    return
+                need = state_bytes(cfg, self.precision)
+                self.budget.acquire(need)
+                try:
+                    with torch.cuda.device(self.device), torch.cuda.stream(stream):
+                        results[i] = run_model(cfg, steps, self.device, self.precision,
+                                               self.max_blocks, self.dc_cycle, keep)
+                        stream.synchronize()
+                except Exception as e:   # reported after all workers stop
+                    errors.append((i, e))
+                finally:
+                    self.budget.release(need)
+
+        threads = [threading.Thread(target=worker, daemon=True) for _ in range(self.concurrency)]
+        for th in threads:
+            th.start()
+        for th in threads:
+            th.join()
+        wall = time.perf_counter() - t0
+        if errors:
+            i, e = errors[0]
+            raise RuntimeError("model %d failed: %s" % (i, e)) from e
+        updates = sum(r["cell_updates"] for r in results)
+        return results, {"wall_s": wall, "cell_updates": updates,
+                         "cell_updates_per_s": updates / wall if wall > 0 else 0.0,
+                         "models": len(results), "concurrency": self.concurrency,
+                         "max_blocks": self.max_blocks}

@@ -97,8 +97,9 @@ class Model:
         """Call tse_<name> or its mixed-precision form tse_<name>_dc."""
         L = N.lib()
         if self.precision == "fp32dc" and conv >= getattr(self, "dc_min_conv", self.DC_MIN_CONV):
+            opts = N.TseDcOptions(self.dc_cycle, getattr(self, "max_blocks", 0))
             rc = getattr(L, "tse_%s_dc" % name)(ct.byref(self.grid), ct.byref(args_struct),
-                                                self.dc_cycle, self._p(self.status),
+                                                ct.byref(opts), self._p(self.status),
                                                 self._p(self.ws), self.ws_bytes, self._stream())
         else:
             rc = getattr(L, "tse_" + name)(ct.byref(self.grid), ct.byref(args_struct),
