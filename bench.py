@@ -37,6 +37,12 @@ sys.path.insert(0, HERE)
 # algorithmic bytes per pressure cell-update (coefficient form, neighbour
 # reuse from cache): FP64 57 B, FP32 29 B
 ALG_BYTES = {"fp64": 57, "fp32dc": 29}
+# DRAM bytes per cell-update measured by ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum over one launch / its cell-updates), from
+# profiles/dc_sweep_kernel_reservoir_192x192x128.md and
+# profiles/rb_solve_kernel_fp64_reservoir_192x192x128.md; scaled to a launch
+# of the benchmark by its cell-updates
+TRAFFIC_BYTES = {"fp32dc": 34.0, "fp64": 114.4}
 DEFAULT_SHAPE = (256, 256, 128)
 
 
@@ -270,7 +276,7 @@ def timed_steps(ctx, sim, steps, clocks=None):
     torch = ctx.torch
     M = sim.M
     cu0 = dict(M.cell_updates)
-    M.timing, M.timed = True, []
+    M.timing, M.timed, M.sweep_timed = True, [], []
     launches0 = M.launches
     if clocks:
         clocks.start()
@@ -285,14 +291,24 @@ def timed_steps(ctx, sim, steps, clocks=None):
     M.timing = False
     ms = e0.elapsed_time(e1)
     updates = sum(M.cell_updates[k] - cu0[k] for k in cu0)
-    p_units, p_ms, n_p = 0.0, 0.0, 0
+    p_units, p_ms, n_p, active_p = 0.0, 0.0, 0, 0
     for kind, s0, s1, nit, active in M.timed:
         if kind == "P":
             p_units += float(nit) * active
             p_ms += s0.elapsed_time(s1)
             n_p += 1
+            active_p = active
+    # mixed-precision form: the FP32 sweep kernel's own launches (events
+    # recorded by the library around each launch on the solve's stream)
+    s_units, s_ms, n_s = 0.0, 0.0, 0
+    for kind, launches, iters, sms in M.sweep_timed:
+        if kind == "P":
+            s_units += float(iters) * active_p
+            s_ms += sms
+            n_s += launches
     return {"ms": ms, "updates": updates, "launches": M.launches - launches0, "clocks": clk,
-            "p_units": p_units, "p_ms": p_ms, "n_p": n_p}
+            "p_units": p_units, "p_ms": p_ms, "n_p": n_p,
+            "s_units": s_units, "s_ms": s_ms, "n_s": n_s}
 
 
 def e2e_steps(ctx, sim, steps):
@@ -324,27 +340,29 @@ def e2e_steps(ctx, sim, steps):
             "d2h_bytes_per_step": int(d2h)}
 
 
-def roofline(res, precision, peak, peak_kind, traffic=None):
-    if not res["n_p"]:
-        return None
-    achieved = res["p_units"] * ALG_BYTES[precision] / (res["p_ms"] / 1e3) / 1e9
-    name = {"fp32dc": "dc_solve_kernel<PressureForm> (FP32 sweeps + FP64 residual)",
-            "fp64": "rb_solve_kernel<PressureForm> (FP64, reference operation order)"}[precision]
+def roofline(res, precision, peak, peak_kind):
+    """Roofline of the dominant kernel: algorithmic bytes / event time.
+    fp32dc: the FP32 sweep kernel (dc_sweep_kernel, 96 % of device time);
+    fp64: the persistent FP64 solve (rb_solve_kernel, one launch per solve,
+    timed with its assembly and unpack kernels)."""
+    if precision == "fp32dc":
+        if not res["n_s"]:
+            return None
+        units, ms, n = res["s_units"], res["s_ms"], res["n_s"]
+        name = "dc_sweep_kernel (FP32 correction sweeps)"
+    else:
+        if not res["n_p"]:
+            return None
+        units, ms, n = res["p_units"], res["p_ms"], res["n_p"]
+        name = "rb_solve_kernel<PressureForm> (FP64, reference operation order)"
+    achieved = units * ALG_BYTES[precision] / (ms / 1e3) / 1e9
+    per_launch = units / n
     return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-            "frac": achieved / peak, "traffic": traffic, "kernel": name,
-            "algorithmic_bytes_per_cell_update": ALG_BYTES[precision],
-            "cell_updates_per_launch": res["p_units"] / res["n_p"],
-            "peak_source": peak_kind, "launches": res["n_p"]}
-
-
-def load_traffic(precision):
-    """DRAM bytes per cell-update of the pressure kernel from the committed ncu
-    summary (profiles/traffic.json), scaled to one launch by the caller."""
-    try:
-        with open(os.path.join(HERE, "profiles", "traffic.json")) as f:
-            return json.load(f).get(precision)
-    except Exception:
-        return None
+            "frac": achieved / peak, "traffic": TRAFFIC_BYTES[precision] * per_launch,
+            "kernel": name, "algorithmic_bytes_per_cell_update": ALG_BYTES[precision],
+            "traffic_bytes_per_cell_update": TRAFFIC_BYTES[precision],
+            "cell_updates_per_launch": per_launch, "launches": n,
+            "ms_per_launch": ms / n, "peak_source": peak_kind}
 
 
 def kernel_only(a):
@@ -446,10 +464,7 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu:
         cpu = cpu_pressure_rate(shape, a.cpu_seconds)
-    tr = load_traffic("fp32dc")
     roof = roofline(res, "fp32dc", peak, peak_kind)
-    if roof and tr:
-        roof["traffic"] = tr * roof["cell_updates_per_launch"]
     if rank == 0:
         print(json.dumps({
             "metric": "SOR cell-updates/s", "value": value, "unit": "cell-updates/s",

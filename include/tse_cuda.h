@@ -139,20 +139,25 @@ int32_t tse_compute_P(const TseGrid *grid, const TsePressureArgs *args,
  * sweep kernel's event record) and return when the solve is done.
  * Workspace: TSE_WS_PRESSURE_DC / TSE_WS_TRANSPORT_DC. */
 typedef struct TseDcOptions {
-    int32_t cycle;       /* iterations per correction cycle, <= 0: 128 */
-    int32_t max_blocks;  /* cap on the sweep kernel's blocks, <= 0: as many as
-                            fit; lets several solves share the GPU at once */
+    int32_t cycle;            /* in: iterations per correction cycle, <= 0: 128 */
+    int32_t max_blocks;       /* in: cap on the sweep kernel's blocks, <= 0: as
+                                 many as fit; lets several solves share the GPU */
+    int32_t timing;           /* in: 1 = time the sweep-kernel launches with
+                                 CUDA events on the call's stream */
+    int32_t sweep_launches;   /* out (timing): sweep-kernel launches */
+    int64_t sweep_iterations; /* out (timing): red+black iterations they ran */
+    double sweep_ms;          /* out (timing): their summed event time */
 } TseDcOptions;
 int32_t tse_compute_P_dc(const TseGrid *grid, const TsePressureArgs *args,
-                         const TseDcOptions *opts, TseSolveStatus *d_status,
+                         TseDcOptions *opts, TseSolveStatus *d_status,
                          void *d_workspace, size_t workspace_bytes,
                          void *stream);
 int32_t tse_compute_C_dc(const TseGrid *grid, const TseSpeciesArgs *args,
-                         const TseDcOptions *opts, TseSolveStatus *d_status,
+                         TseDcOptions *opts, TseSolveStatus *d_status,
                          void *d_workspace, size_t workspace_bytes,
                          void *stream);
 int32_t tse_compute_T_dc(const TseGrid *grid, const TseHeatArgs *args,
-                         const TseDcOptions *opts, TseSolveStatus *d_status,
+                         TseDcOptions *opts, TseSolveStatus *d_status,
                          void *d_workspace, size_t workspace_bytes,
                          void *stream);
 

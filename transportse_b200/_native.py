@@ -65,7 +65,9 @@ class TseHeatArgs(ct.Structure):
 
 
 class TseDcOptions(ct.Structure):
-    _fields_ = [("cycle", ct.c_int32), ("max_blocks", ct.c_int32)]
+    _fields_ = [("cycle", ct.c_int32), ("max_blocks", ct.c_int32), ("timing", ct.c_int32),
+                ("sweep_launches", ct.c_int32), ("sweep_iterations", ct.c_int64),
+                ("sweep_ms", ct.c_double)]
 
 
 # name -> (restype, argtypes)

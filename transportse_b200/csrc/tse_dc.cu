@@ -38,6 +38,13 @@ constexpr double kRefresh = 1e-4;
 #define TSE_SWEEP_MINB 5   // 48 registers, no spills (measured best of 4/5/6/8)
 #endif
 constexpr int kSweepMinBlocks = TSE_SWEEP_MINB;
+#ifndef TSE_SWEEP_BLOCK
+#define TSE_SWEEP_BLOCK 256
+#endif
+constexpr int kSweepBlock = TSE_SWEEP_BLOCK;
+#ifndef TSE_SWEEP_CHUNKED
+#define TSE_SWEEP_CHUNKED 0   // 1: contiguous chunks with neighbour-only phase sync
+#endif
 constexpr int kResBlocks = 2048;   // fixed grid of the residual kernel (deterministic sums)
 
 // events that end a sweep launch
@@ -71,6 +78,9 @@ struct DcCtl {
     double* partials;    // sweep kernel: 4 per block; residual kernel: 1 per block
     GridBarrier* bar;
     DcState* st;
+    long long chunk;     // chunked sweep: compact cells per block
+    int R;               // chunked sweep: PhaseSync neighbour radius
+    unsigned* prog;      // chunked sweep: PhaseSync counters
 };
 
 // ------------------------------------------------------------ FP64 kernels
@@ -205,7 +215,7 @@ __device__ __forceinline__ double reduce_slot(const double* parts, int slot, uns
                                               double* s_val) {
     double s = 0.0;
     for (unsigned b = threadIdx.x; b < nb; b += blockDim.x) s = s + __ldcg(parts + 4 * b + slot);
-    s = block_sum<kBlock>(s, sh);
+    s = block_sum<kSweepBlock>(s, sh);
     if (threadIdx.x == 0) *s_val = s;
     __syncthreads();
     const double r = *s_val;
@@ -218,15 +228,25 @@ __device__ __forceinline__ double reduce_slot(const double* parts, int slot, uns
 // blocks streaming one narrow window of memory; colour phases are separated
 // by the grid barrier.  Per-block partial sums alternate between two slot
 // pairs by check parity, so a slot is rewritten only after a further barrier.
-__global__ void __launch_bounds__(kBlock, kSweepMinBlocks) dc_sweep_kernel(DcCtl c) {
-    __shared__ double sh[kBlock / 32];
+__global__ void __launch_bounds__(kSweepBlock, kSweepMinBlocks) dc_sweep_kernel(DcCtl c) {
+    __shared__ double sh[kSweepBlock / 32];
     __shared__ double s_val;
     const unsigned nb = gridDim.x;
     const long long Nc = c.L.Nc, N = c.Ncal, SX = c.L.SX;
     const int H = c.L.H;
-    const long long step = (long long)nb * blockDim.x;
     const int lane = threadIdx.x & 31;
+#if TSE_SWEEP_CHUNKED
+    // contiguous chunk per block, colour phases ordered by neighbour flags
+    const long long chunk0 = (long long)blockIdx.x * c.chunk;
+    const long long end = chunk0 + c.chunk < Nc ? chunk0 + c.chunk : Nc;
+    const long long step = blockDim.x;
+    const long long w0 = chunk0 + threadIdx.x - lane;
+    PhaseSync sync{c.bar, c.prog, nb, c.R, 0u};
+#else
+    const long long end = Nc;
+    const long long step = (long long)nb * blockDim.x;
     const long long w0 = (long long)blockIdx.x * blockDim.x + threadIdx.x - lane;
+#endif
     const bool leader = (blockIdx.x == 0 && threadIdx.x == 0);
     const float sor = c.sor;
     DcState* st = c.st;
@@ -253,13 +273,13 @@ __global__ void __launch_bounds__(kBlock, kSweepMinBlocks) dc_sweep_kernel(DcCtl
             // all-zero coefficients and r' = 0 and stay at d = 0.  Trips are
             // counted per warp so every lane joins the shuffles; lanes past
             // the end load a valid cell and store nothing.
-            for (long long w = w0; w < Nc; w += step) {
+            for (long long w = w0; w < end; w += step) {
                 const long long ma = w + lane;
-                const bool va = ma < Nc;
-                const long long la = va ? ma : Nc - 1;
+                const bool va = ma < end;
+                const long long la = va ? ma : end - 1;
                 Cell a;
                 load_cell(a, Kc, dw, dq, msk, la, N, SX, H);
-                const float na = relax(a, dq, la, Nc, sor);
+                const float na = relax(a, dq, la, end, sor);
                 if (va) {
                     dw[ma] = na;
                     const float ch = na - a.old;
@@ -268,14 +288,18 @@ __global__ void __launch_bounds__(kBlock, kSweepMinBlocks) dc_sweep_kernel(DcCtl
                 }
             }
             if (col == 1 && check) {
-                const double b1 = block_sum<kBlock>((double)d2, sh);
-                const double b3 = block_sum<kBlock>((double)dd, sh);
+                const double b1 = block_sum<kSweepBlock>((double)d2, sh);
+                const double b3 = block_sum<kSweepBlock>((double)dd, sh);
                 if (threadIdx.x == 0) {
                     c.partials[4 * blockIdx.x + 2 * (checkno & 1)] = b1;
                     c.partials[4 * blockIdx.x + 2 * (checkno & 1) + 1] = b3;
                 }
             }
+#if TSE_SWEEP_CHUNKED
+            ok = (col == 1 && check) ? sync.global() : sync.local();
+#else
             ok = grid_sync(c.bar, nb);
+#endif
         }
         if (!ok) { event = EV_ERROR; break; }
         diff = 1e100;
@@ -349,7 +373,7 @@ static long long dc_delta_len(const Layout& L, long long Ncal) { return Ncal + 2
 size_t dc_extra_bytes(const Layout& L) {
     long long Ncal = (L.Nc + 31) & ~31LL;
     return 2 * ((size_t)7 * Ncal + (size_t)dc_delta_len(L, Ncal)) * sizeof(float) +
-           align256(sizeof(DcState)) + 512;
+           align256(sizeof(DcState)) + align256((size_t)kMaxBlocks * sizeof(unsigned)) + 512;
 }
 
 static int sweep_blocks(long long Nc, int cap) {
@@ -358,11 +382,11 @@ static int sweep_blocks(long long Nc, int cap) {
     cudaGetDevice(&dev);
     if (dev != cached_dev) {
         cudaDeviceGetAttribute(&cached_sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cached_per_sm, dc_sweep_kernel, kBlock, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&cached_per_sm, dc_sweep_kernel, kSweepBlock, 0);
         cached_dev = dev;
     }
     long long maxb = (long long)cached_sms * (cached_per_sm > 0 ? cached_per_sm : 1);
-    long long want = (Nc + (long long)kBlock * 4 - 1) / ((long long)kBlock * 4);
+    long long want = (Nc + (long long)kSweepBlock * 4 - 1) / ((long long)kSweepBlock * 4);
     if (want < 1) want = 1;
     long long nb = want < maxb ? want : maxb;
     // the setup's partials region holds 2 * kMaxBlocks doubles
@@ -374,7 +398,7 @@ static int sweep_blocks(long long Nc, int cap) {
 template <class Form>
 static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, double min_dt,
                   double conv, int max_it, int pressure_schedule, int stop_on_first,
-                  const TseDcOptions* opts, double sor, int x_index, double* X_out,
+                  TseDcOptions* opts, double sor, int x_index, double* X_out,
                   TseSolveStatus* d_status, cudaStream_t stream) {
     const int cycle = opts ? opts->cycle : 0;
     const int cap = opts ? opts->max_blocks : 0;
@@ -403,6 +427,7 @@ static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, 
     c.D[0] = dbase + G;
     c.D[1] = dbase + dlen + G;
     c.st = (DcState*)(dbase + 2 * dlen);
+    c.prog = (unsigned*)((char*)c.st + align256(sizeof(DcState)));
     c.partials = S.partials;
     c.bar = S.bar;
     DcState init;
@@ -416,33 +441,73 @@ static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, 
     const long long cells2 = 2 * S.L.Nc;
     const unsigned gcells = (unsigned)((cells2 + kBlock - 1) / kBlock);
     const int nb = sweep_blocks(S.L.Nc, cap);
+    c.chunk = (S.L.Nc + nb - 1) / nb;
+    c.R = neighbour_radius(S.L.SX, c.chunk, (unsigned)nb);
     dc_scale_kernel<<<gcells, kBlock, 0, stream>>>(S.F, c);
     if (cudaGetLastError() != cudaSuccess) return TSE_ERR_LAUNCH;
+    const bool timing = opts && opts->timing;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    if (timing) {
+        opts->sweep_launches = 0;
+        opts->sweep_iterations = 0;
+        opts->sweep_ms = 0.0;
+        if (cudaEventCreate(&ev0) != cudaSuccess || cudaEventCreate(&ev1) != cudaSuccess)
+            return TSE_ERR_LAUNCH;
+    }
+    int prev_it = 0;
+    int rc = TSE_OK;
     for (;;) {
         const unsigned rb = (unsigned)std::min<long long>(kResBlocks, (cells2 + kBlock - 1) / kBlock);
         dc_residual_kernel<<<rb, kBlock, 0, stream>>>(S.F, c);
         dc_x2_kernel<<<1, kBlock, 0, stream>>>(c, (int)rb);
         void* args[] = {(void*)&c};
+        if (TSE_SWEEP_CHUNKED &&
+            cudaMemsetAsync(c.prog, 0, (size_t)nb * sizeof(unsigned), stream) != cudaSuccess) {
+            rc = TSE_ERR_LAUNCH;
+            break;
+        }
+        if (timing) cudaEventRecord(ev0, stream);
         if (cudaGetLastError() != cudaSuccess ||
-            cudaLaunchCooperativeKernel((const void*)dc_sweep_kernel, dim3(nb), dim3(kBlock), args, 0,
-                                        stream) != cudaSuccess)
-            return TSE_ERR_LAUNCH;
-        int event = EV_ERROR;
-        if (cudaMemcpyAsync(&event, &c.st->event, sizeof(int), cudaMemcpyDeviceToHost, stream) !=
+            cudaLaunchCooperativeKernel((const void*)dc_sweep_kernel, dim3(nb), dim3(kSweepBlock), args,
+                                        0, stream) != cudaSuccess) {
+            rc = TSE_ERR_LAUNCH;
+            break;
+        }
+        if (timing) cudaEventRecord(ev1, stream);
+        int head[2] = {EV_ERROR, 0};   // event, num_it
+        if (cudaMemcpyAsync(&head[0], &c.st->event, sizeof(int), cudaMemcpyDeviceToHost, stream) !=
                 cudaSuccess ||
-            cudaStreamSynchronize(stream) != cudaSuccess)
-            return TSE_ERR_LAUNCH;
+            cudaMemcpyAsync(&head[1], &c.st->num_it, sizeof(int), cudaMemcpyDeviceToHost, stream) !=
+                cudaSuccess ||
+            cudaStreamSynchronize(stream) != cudaSuccess) {
+            rc = TSE_ERR_LAUNCH;
+            break;
+        }
+        const int event = head[0];
+        if (timing) {
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, ev0, ev1);
+            opts->sweep_launches += 1;
+            opts->sweep_iterations += head[1] - prev_it;
+            opts->sweep_ms += ms;
+        }
+        prev_it = head[1];
         if (event == EV_HALVE || event == EV_STOP_HALVED) {
             dc_halve_kernel<<<gcells, kBlock, 0, stream>>>(S.F, c);
-            if (cudaGetLastError() != cudaSuccess) return TSE_ERR_LAUNCH;
+            if (cudaGetLastError() != cudaSuccess) { rc = TSE_ERR_LAUNCH; break; }
             if (event == EV_STOP_HALVED) break;
             continue;
         }
         if (event == EV_ERROR) break;
         dc_apply_kernel<<<gcells, kBlock, 0, stream>>>(c);
-        if (cudaGetLastError() != cudaSuccess) return TSE_ERR_LAUNCH;
+        if (cudaGetLastError() != cudaSuccess) { rc = TSE_ERR_LAUNCH; break; }
         if (event == EV_CONVERGED || event == EV_STOP) break;
     }
+    if (timing) {
+        cudaEventDestroy(ev0);
+        cudaEventDestroy(ev1);
+    }
+    if (rc != TSE_OK) return rc;
     dc_status_kernel<<<1, 1, 0, stream>>>(c.st, d_status);
     if (cudaGetLastError() != cudaSuccess) return TSE_ERR_LAUNCH;
     return launch_unpack(X_out, c.X[0], c.X[1], S.L, stream);
@@ -453,7 +518,7 @@ static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, 
 using namespace tse;
 
 extern "C" int32_t tse_compute_P_dc(const TseGrid* grid, const TsePressureArgs* args,
-                                    const TseDcOptions* opts,
+                                    TseDcOptions* opts,
                                     TseSolveStatus* d_status, void* d_ws, size_t ws_bytes,
                                     void* stream_) {
     if (!grid || !args || !d_status || !d_ws) return TSE_ERR_ARG;
@@ -470,7 +535,7 @@ extern "C" int32_t tse_compute_P_dc(const TseGrid* grid, const TsePressureArgs* 
 }
 
 extern "C" int32_t tse_compute_C_dc(const TseGrid* grid, const TseSpeciesArgs* a,
-                                    const TseDcOptions* opts,
+                                    TseDcOptions* opts,
                                     TseSolveStatus* d_status, void* d_ws, size_t ws_bytes,
                                     void* stream_) {
     if (!grid || !a || !d_status || !d_ws) return TSE_ERR_ARG;
@@ -487,7 +552,7 @@ extern "C" int32_t tse_compute_C_dc(const TseGrid* grid, const TseSpeciesArgs* a
 }
 
 extern "C" int32_t tse_compute_T_dc(const TseGrid* grid, const TseHeatArgs* a,
-                                    const TseDcOptions* opts,
+                                    TseDcOptions* opts,
                                     TseSolveStatus* d_status, void* d_ws, size_t ws_bytes,
                                     void* stream_) {
     if (!grid || !a || !d_status || !d_ws) return TSE_ERR_ARG;

@@ -78,6 +78,7 @@ class Model:
         # status) appended by the solver entry points when enabled
         self.timing = False
         self.timed = []
+        self.sweep_timed = []
         # cell-updates = active cells relaxed once per red+black iteration
         self.cell_updates = {"P": 0, "C": 0, "T": 0}
 
@@ -97,10 +98,15 @@ class Model:
         """Call tse_<name> or its mixed-precision form tse_<name>_dc."""
         L = N.lib()
         if self.precision == "fp32dc" and conv >= getattr(self, "dc_min_conv", self.DC_MIN_CONV):
-            opts = N.TseDcOptions(self.dc_cycle, getattr(self, "max_blocks", 0))
+            opts = N.TseDcOptions(self.dc_cycle, getattr(self, "max_blocks", 0), int(self.timing))
             rc = getattr(L, "tse_%s_dc" % name)(ct.byref(self.grid), ct.byref(args_struct),
                                                 ct.byref(opts), self._p(self.status),
                                                 self._p(self.ws), self.ws_bytes, self._stream())
+            if self.timing:
+                # per sweep-kernel timing of this solve: (kind, launches,
+                # red+black iterations, event ms)
+                self.sweep_timed.append((name[-1], opts.sweep_launches, opts.sweep_iterations,
+                                         opts.sweep_ms))
         else:
             rc = getattr(L, "tse_" + name)(ct.byref(self.grid), ct.byref(args_struct),
                                            self._p(self.status), self._p(self.ws), self.ws_bytes,
