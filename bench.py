@@ -38,10 +38,9 @@ sys.path.insert(0, HERE)
 # reuse from cache): FP64 57 B, FP32 29 B
 ALG_BYTES = {"fp64": 57, "fp32dc": 29}
 # DRAM bytes per cell-update measured by ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum over one launch / its cell-updates), from
-# profiles/dc_sweep_kernel_reservoir_192x192x128.md and
-# profiles/rb_solve_kernel_fp64_reservoir_192x192x128.md; scaled to a launch
-# of the benchmark by its cell-updates
+# dram__bytes_write.sum of one 64-iteration launch on the 192x192x128
+# reservoir, divided by its cell-updates; summaries under profiles/), scaled
+# to a launch of the benchmark by its cell-updates
 TRAFFIC_BYTES = {"fp32dc": 34.0, "fp64": 114.4}
 DEFAULT_SHAPE = (256, 256, 128)
 
@@ -62,7 +61,7 @@ def parse_args():
                          "(for isolated kernel timing and profiler captures)")
     ap.add_argument("--iters", type=int, default=200)
     ap.add_argument("--repeat", type=int, default=3)
-    ap.add_argument("--workload", choices=("reservoir", "ensemble", "serving"),
+    ap.add_argument("--workload", choices=("reservoir", "ensemble", "serving", "sloped"),
                     default="reservoir")
     ap.add_argument("--models", type=int, default=48, help="ensemble: models")
     ap.add_argument("--n-max", type=int, default=None, help="ensemble/serving: largest axis")
@@ -103,6 +102,55 @@ def bench_ensemble(a):
                    "cells_total": int(sum(cells)), "cells_max": int(max(cells))},
         "wall_s": st["wall_s"], "concurrency": conc, "dc_cycle": cyc, "max_blocks": st["max_blocks"],
         "autotune": tune, "clocks": clk}))
+
+
+def bench_sloped(a):
+    """Large sloped model (sloped_3d: beta 5 deg, anisotropic lognormal K, three
+    species with dispersivity 10/1 m, Smolarkiewicz correction, NLTE heat,
+    SIA), FP32+DC with FP64 mass-balance totals, against an FP64 GPU run of the
+    same steps."""
+    import numpy
+    import torch
+    from transportse_b200 import workloads
+    from transportse_b200.driver import Simulation
+    dev = torch.device("cuda:0")
+    shape = tuple(int(x) for x in a.shape.lower().split("x")) if a.shape else (512, 512, 256)
+    cfg = workloads.sloped_3d(*shape)
+    cfg.GPU_MASSBAL = True
+    out = {}
+    fields = {}
+    for prec in ("fp32dc", "fp64"):
+        sim = Simulation(cfg, device=dev, precision=prec)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        cu0 = sum(sim.M.cell_updates.values())
+        e0.record()
+        sim.run(max_steps=a.steps)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        cu = sum(sim.M.cell_updates.values()) - cu0
+        out[prec] = {"ms_per_step": ms / a.steps, "cell_updates_per_s": cu / (ms / 1e3),
+                     "iterations": dict(sim.counters),
+                     "mass": {k: (v.tolist() if hasattr(v, "tolist") else v)
+                              for k, v in sim.mass_log[-1].items()}}
+        fields[prec] = {n: sim.field(n) for n in ("P", "C", "T")}
+        del sim
+        torch.cuda.empty_cache()
+    err = {n: float(numpy.max(numpy.abs(fields["fp32dc"][n] - fields["fp64"][n]))
+                    / max(numpy.max(numpy.abs(fields["fp64"][n])), 1e-300)) for n in ("P", "C", "T")}
+    m32, m64 = out["fp32dc"]["mass"], out["fp64"]["mass"]
+    mass_rel = {"water": abs(m32["water"] - m64["water"]) / abs(m64["water"]),
+                "heat": abs(m32["heat"] - m64["heat"]) / abs(m64["heat"]),
+                "species": [abs(x - y) / max(abs(y), 1e-300)
+                            for x, y in zip(m32["species"], m64["species"])]}
+    print(json.dumps({
+        "metric": "SOR cell-updates/s", "value": out["fp32dc"]["cell_updates_per_s"],
+        "unit": "cell-updates/s", "n_gpus": 1, "steps": a.steps, "higher_is_better": True,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "sloped_3d %dx%dx%d, %d SIA steps, FP32+DC vs FP64" % (shape + (a.steps,))},
+        "fp32dc": out["fp32dc"], "fp64": out["fp64"], "max_rel_err_vs_fp64": err,
+        "mass_rel_diff_vs_fp64": mass_rel}))
 
 
 def bench_serving(a):
@@ -418,6 +466,8 @@ def main():
         return bench_ensemble(a)
     if a.workload == "serving":
         return bench_serving(a)
+    if a.workload == "sloped":
+        return bench_sloped(a)
     import numpy
     import torch
     import torch.distributed as dist

@@ -263,6 +263,25 @@ int32_t tse_peclet_T(const TseGrid *grid, const double *qx, const double *qy,
                      const double *BT, double *d_out, void *d_workspace,
                      size_t workspace_bytes, void *stream);
 
+/* Mass-balance totals in FP64 (no counterpart kernel in the reference, whose
+ * mass_balance is a user callback, tse.py:1460-1463): d_out receives, with
+ * V = dx dy dz per cell,
+ *   [0]            water   sum phi rho_f V
+ *   [1..ns]        species sum RC phi C_s V
+ *   [ns+1]         heat    sum (phi rho_f cp_f + (1-phi) rho_r cp_r) T V
+ *   [ns+2]         source rate sum WP V
+ *   [ns+3..2ns+2]  source rates sum WC_s V
+ *   [2ns+3]        source rate sum WT V
+ * h_C / h_WC are HOST arrays of nspec (<= 8) device pointers; workspace
+ * TSE_WS_REDUCE. */
+int32_t tse_mass_totals(const TseGrid *grid, const double *phi,
+                        const double *rho_f, const double *RC,
+                        const double *const *h_C, const double *const *h_WC,
+                        int32_t nspec, const double *T, const double *cp_f,
+                        const double *rho_r, const double *cp_r,
+                        const double *WP, const double *WT, double *d_out,
+                        void *d_workspace, size_t workspace_bytes, void *stream);
+
 /* Library version string. */
 const char *tse_version(void);
 

@@ -127,3 +127,25 @@ def test_reductions_vs_oracle(cuda_device):
     assert m.explicit_C(D4, phi) == orc.explicit_C(D4, phi)
     s, mx, mn = m.field_stats(a)
     assert mx == a.max() and mn == a.min() and abs(s - a.sum()) <= 1e-12 * numpy.abs(a).sum()
+
+
+def test_mass_totals_vs_numpy(cuda_device):
+    """FP64 device mass-balance totals against a NumPy FP64 evaluation."""
+    from transportse_b200 import workloads
+    from transportse_b200.driver import Simulation
+    cfg = workloads.reservoir_3d(14, 9, 11, seed=3)
+    cfg.GPU_MASSBAL = True
+    sim = Simulation(cfg, device=cuda_device).run(max_steps=2)
+    last = sim.mass_log[-1]
+    f = sim.field
+    V = (cfg.dx[:, None, None] * cfg.dy[None, :, None] * cfg.dz[None, None, :])
+    phi, rho = f("phi"), f("rho_f")
+    water = numpy.sum(phi * rho * V)
+    C = f("C")
+    species = [numpy.sum(f("R") * phi * C[..., s] * V) for s in range(C.shape[-1])]
+    heat = numpy.sum((phi * rho * f("cp_f") + (1 - phi) * f("rho_r") * f("cp_r")) * f("T") * V)
+    assert abs(last["water"] - water) <= 1e-12 * abs(water)
+    for s in range(C.shape[-1]):
+        assert abs(last["species"][s] - species[s]) <= 1e-12 * abs(species[s])
+    assert abs(last["heat"] - heat) <= 1e-12 * abs(heat)
+    assert len(sim.mass_log) == 2

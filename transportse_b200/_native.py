@@ -99,6 +99,8 @@ SIGNATURES = {
     "tse_eos_linear": (_I, [_G, _PP, ct.POINTER(ct.c_int32), _dp, _I, _P, _D, _D, _D, _P, _P]),
     "tse_peclet_C": (_I, [_G, _P, _P, _P, _PP, _PP, _PP, _I, _P, _P, _P, _S, _P]),
     "tse_peclet_T": (_I, [_G, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _S, _P]),
+    "tse_mass_totals": (_I, [_G, _P, _P, _P, _PP, _PP, _I, _P, _P, _P, _P, _P, _P, _P, _P, _S,
+                             _P]),
     "tse_version": (ct.c_char_p, []),
 }
 

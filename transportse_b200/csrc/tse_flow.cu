@@ -272,6 +272,57 @@ __global__ void peclet_t_partial_kernel(TseGrid g, const double* qx, const doubl
     }
 }
 
+// Mass-balance totals in FP64 (cell volume V = dx dy dz):
+//   water  sum phi rho V             species s  sum RC phi C_s V
+//   heat   sum (phi rho cp_f + (1-phi) rho_r cp_r) T V
+//   source rates  sum WP V, sum WC_s V, sum WT V
+// out (per block partial q): 0 water, 1..ns species, ns+1 heat, ns+2 WP,
+// ns+3..2ns+2 WC, 2ns+3 WT
+struct MassArgs {
+    const double *phi, *rho, *RC, *T, *cp_f, *rho_r, *cp_r, *WP, *WT;
+    const double* C[8];
+    const double* WC[8];
+    int ns;
+};
+
+__global__ void mass_partial_kernel(TseGrid g, MassArgs a, double* parts) {
+    __shared__ double sh[kBlock / 32];
+    const long long n = (long long)g.nx * g.ny * g.nz;
+    const int nq = 2 * a.ns + 4;
+    double acc[20];
+    for (int q = 0; q < 20; ++q) acc[q] = 0.0;
+    for (long long f = (long long)blockIdx.x * blockDim.x + threadIdx.x; f < n;
+         f += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        decode(f, g.ny, g.nz, i, j, k);
+        const double V = g.dx[i] * g.dy[j] * g.dz[k];
+        const double ph = a.phi[f];
+        acc[0] += ph * a.rho[f] * V;
+        for (int s = 0; s < a.ns; ++s) {
+            acc[1 + s] += a.RC[f] * ph * a.C[s][f] * V;
+            acc[a.ns + 3 + s] += a.WC[s][f] * V;
+        }
+        acc[a.ns + 1] += (ph * a.rho[f] * a.cp_f[f] + (1 - ph) * a.rho_r[f] * a.cp_r[f]) * a.T[f] * V;
+        acc[a.ns + 2] += a.WP[f] * V;
+        acc[2 * a.ns + 3] += a.WT[f] * V;
+    }
+    for (int q = 0; q < nq; ++q) {
+        const double r = block_sum<kBlock>(acc[q], sh);
+        if (threadIdx.x == 0) parts[q * gridDim.x + blockIdx.x] = r;
+    }
+}
+
+__global__ void mass_finish_kernel(const double* parts, int nparts, int nq, double* out) {
+    __shared__ double sh[kBlock / 32];
+    for (int q = 0; q < nq; ++q) {
+        double v = 0.0;
+        for (int b = threadIdx.x; b < nparts; b += blockDim.x) v = v + parts[q * nparts + b];
+        const double r = block_sum<kBlock>(v, sh);
+        if (threadIdx.x == 0) out[q] = r;
+        __syncthreads();
+    }
+}
+
 // Declared linear EOS: rho = rho0 + a0*C[s0] + ... - tcoef*(T - T0)
 struct EosLinear {
     const double* C[8];
@@ -441,6 +492,42 @@ extern "C" int32_t tse_peclet_T(const TseGrid* grid, const double* qx, const dou
     if (cudaGetLastError() != cudaSuccess) return TSE_ERR_LAUNCH;
     static const int ops[3] = {R_MAX, R_MAX, R_MAX};
     return finish(parts, nb, 3, ops, d_out, 0, ws, s);
+}
+
+extern "C" int32_t tse_mass_totals(const TseGrid* grid, const double* phi, const double* rho_f,
+                                   const double* RC, const double* const* h_C,
+                                   const double* const* h_WC, int32_t nspec, const double* T,
+                                   const double* cp_f, const double* rho_r, const double* cp_r,
+                                   const double* WP, const double* WT, double* d_out, void* ws,
+                                   size_t ws_bytes, void* stream) {
+    if (!grid || !phi || !rho_f || !RC || !T || !cp_f || !rho_r || !cp_r || !WP || !WT || !d_out ||
+        !ws || nspec < 0 || nspec > 8 || (nspec > 0 && (!h_C || !h_WC)))
+        return TSE_ERR_ARG;
+    const long long n = (long long)grid->nx * grid->ny * grid->nz;
+    const int nq = 2 * nspec + 4;
+    const unsigned nb = red_blocks(n) > 256 ? 256 : red_blocks(n);
+    if (ws_bytes < reduce_ws_bytes() || (size_t)nq * nb > (size_t)8 * kRedBlocks) return TSE_ERR_WORKSPACE;
+    MassArgs a;
+    a.phi = phi;
+    a.rho = rho_f;
+    a.RC = RC;
+    a.T = T;
+    a.cp_f = cp_f;
+    a.rho_r = rho_r;
+    a.cp_r = cp_r;
+    a.WP = WP;
+    a.WT = WT;
+    a.ns = nspec;
+    for (int s = 0; s < 8; ++s) {
+        a.C[s] = s < nspec ? h_C[s] : nullptr;
+        a.WC[s] = s < nspec ? h_WC[s] : nullptr;
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    double* parts = (double*)ws;
+    mass_partial_kernel<<<nb, kBlock, 0, s>>>(*grid, a, parts);
+    if (cudaGetLastError() != cudaSuccess) return TSE_ERR_LAUNCH;
+    mass_finish_kernel<<<1, kBlock, 0, s>>>(parts, (int)nb, nq, d_out);
+    return cudaGetLastError() == cudaSuccess ? TSE_OK : TSE_ERR_LAUNCH;
 }
 
 extern "C" int32_t tse_eos_linear(const TseGrid* grid, const double* const* h_C,

@@ -87,6 +87,7 @@ class Simulation:
         self.t_sim = getattr(config, "t_sim", 0)
         self.n_tsteps = 0
         self.log = []
+        self.mass_log = []
         self.counters = dict(P=0, C=0, T=0)
 
     # ------------------------------------------------------------ state I/O
@@ -299,6 +300,8 @@ class Simulation:
             self.log.append(rec)
             if cfg.DYNAMICBC:
                 self._dynamic_bc(dt)
+            if cfg.MASSBALAN or getattr(cfg, "GPU_MASSBAL", False):
+                self._mass_balance(dt)
             if on_step is not None:
                 on_step(rec, self)
             self.t_sim += dt
@@ -343,6 +346,27 @@ class Simulation:
         self._bc_inc = new_inc
         if new_inc != bc_inc and cfg.FLUIDPROP:
             self.update_fluid_properties()
+
+    def _mass_balance(self, dt):
+        """Mass balance at the point of tse.py:1460-1463: FP64 device totals
+        (water, species, heat and their source rates) appended to
+        ``mass_log``; a config's own mass_balance callback, when MASSBALAN is
+        set, is called as the reference calls it, on host copies."""
+        S, cfg = self.S, self.config
+        T0 = S["T"][0] if self.nlte else S["T"]
+        ns = S["C"].shape[0]
+        tot = self.M.mass_totals(S["phi"], S["rho_f"], S["R"], [S["C"][s] for s in range(ns)],
+                                 [S["WC"][s] for s in range(ns)], T0, S["cp_f"], S["rho_r"],
+                                 S["cp_r"], S["WP"], S["WT"])
+        self.mass_log.append({"t": self.t_sim + dt, "dt": dt, "water": tot[0],
+                              "species": tot[1:1 + ns].copy(), "heat": tot[1 + ns],
+                              "water_source": tot[2 + ns], "species_source": tot[3 + ns:3 + 2 * ns].copy(),
+                              "heat_source": tot[3 + 2 * ns]})
+        if cfg.MASSBALAN and hasattr(cfg, "mass_balance"):
+            f = self.field
+            self.mass = cfg.mass_balance(f("C"), f("qx"), f("qy"), f("qz"), f("WP"), f("WC"),
+                                         f("WT"), f("D_fx"), f("D_fy"), f("D_fz"), dt,
+                                         getattr(self, "mass", numpy.array(cfg.mass, copy=True)))
 
     def _halving_log(self, which, s):
         if not self.verbose or s is None or s.n_events == 0:

@@ -356,6 +356,22 @@ class Model:
         v = self.scal[:3].cpu().numpy()
         return float(v[0]), float(v[1]), float(v[2])
 
+    def mass_totals(self, phi, rho_f, RC, C_species, WC_species, T, cp_f, rho_r, cp_r, WP, WT):
+        """FP64 totals: water, species (ns), heat, then the source rates of
+        water, species (ns), heat -- see tse_mass_totals."""
+        ns = len(C_species)
+        mk = lambda L: (ct.c_void_p * max(1, len(L)))(*[x.data_ptr() for x in L])
+        args = [self._t(x) for x in (phi, rho_f, RC)]
+        rest = [self._t(x) for x in (T, cp_f, rho_r, cp_r, WP, WT)]
+        out = torch.zeros(2 * ns + 4, dtype=torch.float64, device=self.device)
+        rc = N.lib().tse_mass_totals(ct.byref(self.grid), *[self._p(x) for x in args],
+                                     mk(C_species), mk(WC_species), ns,
+                                     *[self._p(x) for x in rest], self._p(out),
+                                     self._p(self.red_ws), self.red_ws.numel(), self._stream())
+        N.check(rc, "tse_mass_totals")
+        self.launches += 2
+        return out.cpu().numpy()
+
     def eos_linear(self, C_species, T, rho_f, rho0, species_coeffs, tcoef, T0):
         """Declared linear EOS: rho_f = rho0 + sum a_s C_s - tcoef (T - T0)."""
         m = len(species_coeffs)
