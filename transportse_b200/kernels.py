@@ -333,6 +333,18 @@ class Model:
         v = self.scal[:3].cpu().numpy()
         return float(v[0]), float(v[1]), float(v[2])
 
+    def sums(self, fields):
+        """FP64 sums of several device fields with one host round trip."""
+        out = torch.empty(3 * len(fields), dtype=torch.float64, device=self.device)
+        for q, x in enumerate(fields):
+            x = self._t(x)
+            rc = N.lib().tse_field_stats(self._p(x), x.numel(), ct.c_void_p(out.data_ptr() + 24 * q),
+                                         self._p(self.red_ws), self.red_ws.numel(), self._stream())
+            N.check(rc, "tse_field_stats")
+            self.launches += 2
+        v = out.cpu().numpy()
+        return [float(v[3 * q]) for q in range(len(fields))]
+
     def peclet_C(self, qx, qy, qz, D_fx, D_fy, D_fz, BC):
         Dx, Dy, Dz = self._species_list(D_fx), self._species_list(D_fy), self._species_list(D_fz)
         mk = lambda L: (ct.c_void_p * len(L))(*[x.data_ptr() for x in L])
