@@ -25,6 +25,10 @@ from __future__ import annotations
 import argparse
 import json
 import os
+
+# concurrent model streams (ensemble / serving workloads) need more than the
+# default eight hardware work queues; must be set before the CUDA context
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 import statistics
 import subprocess
 import sys
@@ -65,7 +69,12 @@ def parse_args():
                     default="reservoir")
     ap.add_argument("--models", type=int, default=48, help="ensemble: models")
     ap.add_argument("--n-max", type=int, default=None, help="ensemble/serving: largest axis")
-    ap.add_argument("--concurrency", type=int, default=0, help="ensemble: 0 = autotune")
+    ap.add_argument("--concurrency", type=int, default=0,
+                    help="ensemble, unbatched: models in flight (0 = autotune)")
+    ap.add_argument("--cluster", type=int, default=0,
+                    help="ensemble/serving, batched: CTAs per model (0 = autotune / 8)")
+    ap.add_argument("--unbatched", action="store_true",
+                    help="ensemble/serving: one solve launch per model instead of batched launches")
     ap.add_argument("--requests", type=int, default=40, help="serving: requests")
     ap.add_argument("--rate", type=float, default=20.0, help="serving: arrivals per second")
     ap.add_argument("--slots", type=int, default=8, help="serving: concurrent models")
@@ -75,7 +84,9 @@ def parse_args():
 def bench_ensemble(a):
     """Ensemble of independent models (log-uniform 32-128 per axis, lognormal
     K, one source/sink, one species plus heat), FP32+DC, a.steps time steps
-    each; concurrency and cycle length autotuned on a sample."""
+    each.  Batched (default): every model resident, each kind of solve of all
+    models in one launch, cluster size autotuned on a sample; unbatched:
+    concurrency and cycle length autotuned on a sample."""
     import torch
     from transportse_b200 import workloads
     from transportse_b200.ensemble import Ensemble, autotune
@@ -83,15 +94,26 @@ def bench_ensemble(a):
     nmax = a.n_max or 128
     cfgs = [workloads.ensemble_member(seed=1000 + i, n_max=nmax) for i in range(a.models)]
     tune = None
-    if a.concurrency <= 0:
-        tune = autotune(cfgs[:8], device=dev, steps=1, concurrency=(2, 4, 8), cycles=(128, 256))
-        conc, cyc = tune["concurrency"], tune["dc_cycle"]
+    batched = not a.unbatched
+    conc = cyc = cl = None
+    if batched:
+        if a.cluster <= 0:
+            tune = autotune(cfgs[:16], device=dev, steps=1, batched=True, clusters=(4, 8, 16),
+                            cycles=(128,))
+            cl = tune["cluster"]
+        else:
+            cl = a.cluster
+        kw = {"batched": True, "cluster": cl}
     else:
-        conc, cyc = a.concurrency, None
+        if a.concurrency <= 0:
+            tune = autotune(cfgs[:8], device=dev, steps=1, concurrency=(2, 4, 8), cycles=(128, 256))
+            conc, cyc = tune["concurrency"], tune["dc_cycle"]
+        else:
+            conc = a.concurrency
+        kw = {"batched": False, "concurrency": conc}
     clocks = ClockSampler(0)
     clocks.start()
-    _, st = Ensemble(cfgs, device=dev, precision="fp32dc", concurrency=conc, dc_cycle=cyc).run(
-        a.steps, keep=())
+    _, st = Ensemble(cfgs, device=dev, precision="fp32dc", dc_cycle=cyc, **kw).run(a.steps, keep=())
     clk = clocks.stop()
     cells = [c.nx * c.ny * c.nz for c in cfgs]
     print(json.dumps({
@@ -100,7 +122,8 @@ def bench_ensemble(a):
         "config": {"workload": "ensemble of %d models, axes log-uniform 32-%d, %d steps each, "
                                "FP32 sweeps + FP64 defect correction" % (a.models, nmax, a.steps),
                    "cells_total": int(sum(cells)), "cells_max": int(max(cells))},
-        "wall_s": st["wall_s"], "concurrency": conc, "dc_cycle": cyc, "max_blocks": st["max_blocks"],
+        "wall_s": st["wall_s"], "batched": batched, "cluster": cl, "concurrency": st["concurrency"],
+        "dc_cycle": cyc, "max_blocks": st["max_blocks"], "batch": st["batch"],
         "autotune": tune, "clocks": clk}))
 
 
@@ -167,7 +190,8 @@ def bench_serving(a):
     budget = min(150e9, torch.cuda.mem_get_info(dev)[0] * 0.85)
     clocks = ClockSampler(0)
     clocks.start()
-    reqs, st = Server(device=dev, slots=a.slots, hbm_budget=budget).replay(trace)
+    reqs, st = Server(device=dev, slots=a.slots, hbm_budget=budget, batched=not a.unbatched,
+                      cluster=a.cluster).replay(trace)
     clk = clocks.stop()
     print(json.dumps({
         "metric": "SOR cell-updates/s", "value": st["cell_updates_per_s"], "unit": "cell-updates/s",
@@ -176,7 +200,8 @@ def bench_serving(a):
                                "%d steps each, %d slots, HBM budget %.0f GB"
                                % (a.requests, a.rate, nmax, a.steps, a.slots, budget / 1e9)},
         "latency_p50_s": st["p50_s"], "latency_p99_s": st["p99_s"], "latency_mean_s": st["mean_s"],
-        "makespan_s": st["makespan_s"], "clocks": clk}))
+        "makespan_s": st["makespan_s"], "batched": st["batched"], "batch": st["batch"],
+        "clocks": clk}))
 
 
 def shape_of(a):

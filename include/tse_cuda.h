@@ -161,6 +161,50 @@ int32_t tse_compute_T_dc(const TseGrid *grid, const TseHeatArgs *args,
                          void *d_workspace, size_t workspace_bytes,
                          void *stream);
 
+/* Batched mixed-precision solves: the compute_P / compute_C / compute_T
+ * calls of n independent models (an ensemble, or the requests a server is
+ * stepping together), run as one persistent launch with one thread-block
+ * cluster per model.  Each item is exactly the single-model call of
+ * tse_compute_*_dc -- its own grid, arguments, status record and workspace
+ * (TSE_WS_PRESSURE_DC / TSE_WS_TRANSPORT_DC; no two items may share one) --
+ * and gets the same results to the solver tolerance.  opts->cycle as for the
+ * single-model form; opts->max_blocks is the cluster size (CTAs per model,
+ * <= 0: 8, at most 16); the timing fields are not written.  d_batch_ws holds
+ * tse_batch_workspace_bytes(n) bytes.  The call returns after queueing the
+ * work on `stream`; nothing is read back.  A non-finite dt or min_dt is
+ * TSE_ERR_ARG.  Replaces n calls of tse.py:647 / 783 / 919. */
+typedef struct TseBatchPressure {
+    const TseGrid *grid;
+    const TsePressureArgs *args;
+    TseSolveStatus *d_status;
+    void *d_workspace;
+    size_t workspace_bytes;
+} TseBatchPressure;
+typedef struct TseBatchSpecies {
+    const TseGrid *grid;
+    const TseSpeciesArgs *args;
+    TseSolveStatus *d_status;
+    void *d_workspace;
+    size_t workspace_bytes;
+} TseBatchSpecies;
+typedef struct TseBatchHeat {
+    const TseGrid *grid;
+    const TseHeatArgs *args;
+    TseSolveStatus *d_status;
+    void *d_workspace;
+    size_t workspace_bytes;
+} TseBatchHeat;
+size_t tse_batch_workspace_bytes(int32_t n);
+int32_t tse_compute_P_dc_batch(const TseBatchPressure *items, int32_t n,
+                               const TseDcOptions *opts, void *d_batch_ws,
+                               size_t batch_ws_bytes, void *stream);
+int32_t tse_compute_C_dc_batch(const TseBatchSpecies *items, int32_t n,
+                               const TseDcOptions *opts, void *d_batch_ws,
+                               size_t batch_ws_bytes, void *stream);
+int32_t tse_compute_T_dc_batch(const TseBatchHeat *items, int32_t n,
+                               const TseDcOptions *opts, void *d_batch_ws,
+                               size_t batch_ws_bytes, void *stream);
+
 /* Pressure solve that allocates nothing and takes no workspace.  It has no
  * counterpart in the reference; it exists for callers that cannot allocate
  * device memory themselves -- a host program whose device memory belongs to

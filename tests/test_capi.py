@@ -47,6 +47,8 @@ STRUCTS = {
     "TseGrid": N.TseGrid, "TseSolveStatus": N.TseSolveStatus,
     "TsePressureArgs": N.TsePressureArgs, "TseSpeciesArgs": N.TseSpeciesArgs,
     "TseHeatArgs": N.TseHeatArgs, "TseDcOptions": N.TseDcOptions,
+    "TseBatchPressure": N.TseBatchPressure, "TseBatchSpecies": N.TseBatchSpecies,
+    "TseBatchHeat": N.TseBatchHeat,
 }
 
 
@@ -74,3 +76,27 @@ def test_ops_fail_loudly_without_library(monkeypatch):
     monkeypatch.setattr(N, "LIB_PATH", "/nonexistent/libtsecuda.so")
     with pytest.raises(RuntimeError):
         N.lib()
+
+
+def test_batch_entry_points_validate_without_gpu():
+    """Argument errors return TSE_ERR_ARG before any device call."""
+    L = N.lib()
+    assert L.tse_batch_workspace_bytes(4) >= 256
+    opts = N.TseDcOptions(128, 8, 0)
+    g = N.TseGrid(8, 8, 8, 0, None, None, None, 9.81, 0.0, 1.0)
+    ws = ct.c_void_p(4096)   # never dereferenced: validation fails first
+    for name, args_t in (("P", N.TsePressureArgs), ("C", N.TseSpeciesArgs), ("T", N.TseHeatArgs)):
+        fn = getattr(L, "tse_compute_%s_dc_batch" % name)
+        Item = N.BATCH_ITEM["compute_" + name]
+        assert fn(None, 1, ct.byref(opts), ws, 1 << 20, None) == -1
+        a = args_t()
+        a.max_it = 10
+        if name == "P":
+            a.dt_P = float("nan")
+        else:
+            a.dt = float("nan")
+        a.min_dt = 1.0
+        items = (Item * 1)(Item(ct.pointer(g), ct.pointer(a), ws, ws, 1 << 20))
+        assert fn(items, 0, ct.byref(opts), ws, 1 << 20, None) == -1
+        # NaN dt would halve forever: refused
+        assert fn(items, 1, ct.byref(opts), ws, 1 << 20, None) == -1

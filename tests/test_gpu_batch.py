@@ -1,0 +1,155 @@
+"""Batched mixed-precision solves (tse_compute_*_dc_batch through BatchGate):
+every model's result in a batch equals its single-model mixed-precision
+solve to 1e-6 and the reference to the same bound; the dt-halving and stop
+paths give the same t / dt / event sequence; cluster sizes 1-16 agree."""
+import threading
+
+import numpy
+import pytest
+import torch
+
+from oracle.oracle import OracleModel
+from tests.golden import cases
+from tests.helpers import NumpyKernels, load, model_for, rel_err
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-6
+
+
+def _run_members(fns, device, cluster=0):
+    """Run fns[i](gate) on threads of their own, each on its own stream, all
+    joined to one gate before any starts (so the first solves batch)."""
+    from transportse_b200.batch import BatchGate
+    gate = BatchGate(device, cluster=cluster)
+    out = [None] * len(fns)
+    errs = []
+    for _ in fns:
+        gate.join()
+
+    def work(i):
+        s = torch.cuda.Stream(device=device)
+        try:
+            with torch.cuda.device(device), torch.cuda.stream(s):
+                out[i] = fns[i](gate)
+                s.synchronize()
+        except Exception as e:  # reported below
+            errs.append(e)
+        finally:
+            gate.leave()
+
+    th = [threading.Thread(target=work, args=(i,)) for i in range(len(fns))]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    if errs:
+        raise errs[0]
+    return out, gate
+
+
+def _pressure_case(shape, seed):
+    from transportse_b200 import workloads
+    nx, ny, nz = shape
+    rng = numpy.random.default_rng(seed)
+    cfg = workloads.base_config("batch", nx, ny, nz, rng.uniform(0.5, 2, nx),
+                                rng.uniform(0.5, 2, ny), rng.uniform(0.5, 2, nz))
+    cfg.beta = 2.0
+    cfg.c_r[:] = 1e-10
+    K = 1e-12 * numpy.exp(rng.standard_normal(shape))
+    args = (4.5e-10 * numpy.ones(shape), rng.uniform(8e-4, 1.2e-3, shape),
+            rng.uniform(995, 1150, shape), rng.uniform(0.05, 0.3, shape), K, K, 0.3 * K)
+    z = numpy.zeros(shape)
+    P = workloads.hydrostatic(cfg) + rng.uniform(-300, 300, shape)
+    BP = numpy.zeros(shape)
+    BP[:, :, -1] = 1
+    WP = numpy.where(rng.uniform(size=shape) < 0.2, rng.uniform(-1e-4, 1e-4, shape), 0.0)
+    return cfg, P, args + (z, z, z, 3600.0, BP, WP)
+
+
+SHAPES = [(33, 17, 21), (1, 1, 40), (16, 16, 16), (9, 1, 31), (40, 30, 24), (5, 7, 3)]
+
+
+@pytest.mark.parametrize("cluster", [0, 1, 4, 16])
+def test_batched_pressure_equals_single_solves(cluster, cuda_device):
+    kw = dict(SOR=1.7, max_it=20000, inc_it=1.25, max_dt=1e5, min_dt=1e-8, P_conv=1e-10)
+    cases_ = [_pressure_case(s, 7 + i) for i, s in enumerate(SHAPES)]
+    single = []
+    for cfg, P, rest in cases_:
+        single.append(NumpyKernels(model_for(cfg, cuda_device, "fp32dc")).compute_P(
+            P.copy(), *rest, **kw))
+
+    def member(i):
+        cfg, P, rest = cases_[i]
+
+        def fn(gate):
+            m = model_for(cfg, cuda_device, "fp32dc")
+            m.batch_gate = gate
+            return NumpyKernels(m).compute_P(P.copy(), *rest, **kw)
+        return fn
+
+    got, gate = _run_members([member(i) for i in range(len(SHAPES))], cuda_device, cluster)
+    st = gate.stats()
+    assert st["solves"]["compute_P"] == len(SHAPES)
+    assert st["launches"]["compute_P"] == 1
+    for i, (g, s) in enumerate(zip(got, single)):
+        cfg, P, rest = cases_[i]
+        assert g[4] == s[4] and g[0] == s[0] and g[1] == s[1], SHAPES[i]
+        assert abs(g[5] - s[5]) <= max(10, 0.05 * s[5]), (SHAPES[i], g[5], s[5])
+        assert rel_err(g[2], s[2]) <= TOL, SHAPES[i]
+        ro = OracleModel(cfg).compute_P(P.copy(), *rest, **kw)
+        assert rel_err(g[2], ro[2]) <= TOL, SHAPES[i]
+
+
+def test_batched_halving_and_stop_follow_the_reference(cuda_device):
+    # unreachable tolerance: every solve halves dt max_it by max_it until it
+    # reaches min_dt, then stops unconverged (tse.py:724-740)
+    kw = dict(SOR=1.7, max_it=25, inc_it=1.25, max_dt=1e5, min_dt=400.0, P_conv=1e-12)
+    cases_ = [_pressure_case(s, 50 + i) for i, s in enumerate(SHAPES[:4])]
+    ref = [OracleModel(cfg).compute_P(P.copy(), *rest, **kw) for cfg, P, rest in cases_]
+
+    def member(i):
+        cfg, P, rest = cases_[i]
+
+        def fn(gate):
+            m = model_for(cfg, cuda_device, "fp32dc")
+            m.batch_gate = gate
+            return NumpyKernels(m).compute_P(P.copy(), *rest, **kw)
+        return fn
+
+    got, _ = _run_members([member(i) for i in range(len(cases_))], cuda_device)
+    for g, r in zip(got, ref):
+        assert not r[4] and not g[4]
+        assert g[0] == r[0] and g[1] == r[1] and g[5] == r[5]
+        assert rel_err(g[2], r[2]) <= TOL
+
+
+def test_batched_unit_calls_match_reference_fixtures(cuda_device):
+    """Both reference unit cases (pressure, fluxes, species, heat, Smolarkiewicz
+    calls) on two threads whose solves batch together."""
+    variants = ["a", "b"]
+
+    def member(v):
+        def fn(gate):
+            cfg, inp = cases.unit_inputs_with_cfg(v)
+            m = model_for(cfg, cuda_device, "fp32dc")
+            m.batch_gate = gate
+            return cases.run_unit_calls(NumpyKernels(m), inp, v)
+        return fn
+
+    got, gate = _run_members([member(v) for v in variants], cuda_device)
+    assert sum(gate.stats()["solves"].values()) > sum(gate.stats()["launches"].values())
+    for v, out in zip(variants, got):
+        fx = load("unit_" + v)
+        for k in fx.files:
+            if not k.startswith("out_"):
+                continue
+            name = k[4:]
+            ref, g = fx[k], out[name]
+            if name.endswith("_scal"):
+                t, dt, conv, nit = g
+                assert conv == ref[2], name
+                assert abs(nit - ref[3]) <= max(10, 0.05 * max(nit, ref[3])), (name, nit, ref[3])
+                if conv:
+                    assert abs(t - ref[0]) <= 1e-12 * abs(ref[0]), name
+            else:
+                assert rel_err(g, ref) <= TOL, (v, name, rel_err(g, ref))

@@ -22,15 +22,27 @@ def _configs():
             for i, s in enumerate(SHAPES)]
 
 
-@pytest.mark.parametrize("precision,tol", [("fp64", 0.0), ("fp32dc", 1e-6)])
-def test_ensemble_alone_equals_mixed(precision, tol, cuda_device):
+@pytest.mark.parametrize("precision,mode,tol", [("fp64", "streams", 0.0),
+                                                 ("fp32dc", "streams", 1e-6),
+                                                 ("fp32dc", "cluster", 1e-6),
+                                                 ("fp32dc", "batched", 1e-6)])
+def test_ensemble_alone_equals_mixed(precision, mode, tol, cuda_device):
+    """alone: one model at a time, whole-GPU solves; mixed: four at a time
+    (streams), four at a time with every solve a single-cluster launch
+    (cluster), or all in lock step through the batch gate (batched)."""
     from transportse_b200.ensemble import Ensemble
     steps = 3
+    batched = mode == "batched"
     alone, _ = Ensemble(_configs(), device=cuda_device, precision=precision,
-                        concurrency=1).run(steps)
+                        concurrency=1, cluster_cells=0).run(steps)
     mixed, stats = Ensemble(_configs(), device=cuda_device, precision=precision,
-                            concurrency=4).run(steps)
+                            concurrency=None if batched else 4, batched=batched,
+                            cluster_cells=(1 << 30) if mode == "cluster" else 0).run(steps)
     assert stats["models"] == len(SHAPES) and stats["cell_updates"] > 0
+    if batched:
+        b = stats["batch"]
+        assert b["solves"]["compute_P"] >= len(SHAPES) * steps
+        assert b["launches"]["compute_P"] < b["solves"]["compute_P"]
     for a, b in zip(alone, mixed):
         for k in ("P", "C", "T"):
             e = rel_err(b[k], a[k])

@@ -108,3 +108,45 @@ def test_shard_balances_and_covers():
     assert flat == list(range(37))
     loads = [sum(sizes[i] for i in p) for p in parts]
     assert max(loads) <= 1.25 * (sum(sizes) / 4) + max(sizes)
+
+
+def test_batch_gate_launches_when_every_member_waits(monkeypatch):
+    """BatchGate: no launch while a member is still between solves; one launch
+    per solve kind once all wait; members that leave release the rest."""
+    import threading
+    import time
+    from transportse_b200 import batch as B
+
+    launched = []
+
+    def fake_launch(self, reqs):
+        launched.append(sorted(r.name for r in reqs))
+
+    monkeypatch.setattr(B.BatchGate, "_launch", fake_launch)
+    monkeypatch.setattr(B.torch.cuda, "current_stream", lambda device=None: None)
+    gate = B.BatchGate("cpu")
+    order = []
+
+    def member(name, delay, solves):
+        try:
+            for _ in range(solves):
+                time.sleep(delay)
+                gate.submit(name, None, None, None, None, 0, 128)
+                order.append(name)
+        finally:
+            gate.leave()
+
+    for _ in range(3):
+        gate.join()   # all three are members before any submits
+    ths = [threading.Thread(target=member, args=a, daemon=True)
+           for a in (("compute_P", 0.0, 2), ("compute_T", 0.05, 2), ("compute_P", 0.1, 1))]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join(timeout=10)
+    assert not any(t.is_alive() for t in ths)
+    # first flush waits for the slowest member: all three solves together
+    assert launched[0] == ["compute_P", "compute_P", "compute_T"]
+    # the rest flush once the third member has left
+    assert sum(len(x) for x in launched) == 5
+    assert gate.members == 0 and gate.running == 0

@@ -70,6 +70,21 @@ class TseDcOptions(ct.Structure):
                 ("sweep_ms", ct.c_double)]
 
 
+def _batch_item(args_type):
+    class Item(ct.Structure):
+        _fields_ = [("grid", ct.POINTER(TseGrid)), ("args", ct.POINTER(args_type)),
+                    ("d_status", ct.c_void_p), ("d_workspace", ct.c_void_p),
+                    ("workspace_bytes", ct.c_size_t)]
+    return Item
+
+
+TseBatchPressure = _batch_item(TsePressureArgs)
+TseBatchSpecies = _batch_item(TseSpeciesArgs)
+TseBatchHeat = _batch_item(TseHeatArgs)
+BATCH_ITEM = {"compute_P": TseBatchPressure, "compute_C": TseBatchSpecies,
+              "compute_T": TseBatchHeat}
+
+
 # name -> (restype, argtypes)
 _P = ct.c_void_p
 _I = ct.c_int32
@@ -87,6 +102,13 @@ SIGNATURES = {
                               _S, _P]),
     "tse_compute_T_dc": (_I, [_G, ct.POINTER(TseHeatArgs), ct.POINTER(TseDcOptions), _P, _P, _S,
                               _P]),
+    "tse_batch_workspace_bytes": (ct.c_size_t, [_I]),
+    "tse_compute_P_dc_batch": (_I, [ct.POINTER(TseBatchPressure), _I, ct.POINTER(TseDcOptions), _P,
+                                    _S, _P]),
+    "tse_compute_C_dc_batch": (_I, [ct.POINTER(TseBatchSpecies), _I, ct.POINTER(TseDcOptions), _P,
+                                    _S, _P]),
+    "tse_compute_T_dc_batch": (_I, [ct.POINTER(TseBatchHeat), _I, ct.POINTER(TseDcOptions), _P, _S,
+                                    _P]),
     "tse_compute_q": (_I, [_G, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "tse_flow_error": (_I, [_G, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _D, _P, _P]),
     "tse_compute_C": (_I, [_G, ct.POINTER(TseSpeciesArgs), _P, _P, _S, _P]),

@@ -1,0 +1,168 @@
+"""Batched solves across models that each run in their own host thread.
+
+Every model of an ensemble (or every request a server is stepping) runs the
+full time-step driver on its own thread and CUDA stream.  When a model
+reaches a mixed-precision pressure / species / heat solve, ``Model._solve``
+hands the call to the ``BatchGate`` it is attached to and waits.  Once every
+live member is waiting at a solve, the gate issues the waiting calls as one
+``tse_compute_*_dc_batch`` launch per solve kind -- one thread-block cluster
+per model, all models of the kind side by side -- and releases the members.
+Members that are between solves keep the gate open (it never launches a
+partial batch while one of them may still arrive), members that finish
+leave, and new ones join between steps: continuous batching.
+
+Ordering: each kind's launch goes on the gate's own stream for that kind,
+which first waits on an event recorded on every member's stream; each
+member's stream then waits on the launch's completion event, so a member's
+later kernels (and its status read) follow its solve.  The launches of
+different kinds overlap on the GPU.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import threading
+from contextlib import contextmanager
+
+import torch
+
+from . import _native as N
+
+KINDS = ("compute_P", "compute_C", "compute_T")
+
+
+class _Request:
+    __slots__ = ("name", "grid", "args", "status", "ws", "ws_bytes", "stream", "cycle", "done",
+                 "error")
+
+    def __init__(self, name, grid, args, status, ws, ws_bytes, stream, cycle):
+        self.name = name
+        self.grid = grid
+        self.args = args
+        self.status = status
+        self.ws = ws
+        self.ws_bytes = ws_bytes
+        self.stream = stream
+        self.cycle = cycle
+        self.done = False
+        self.error = None
+
+
+class BatchGate:
+    """Collects the mixed-precision solves of the member models and launches
+    them together.  ``cluster``: CTAs per model (0: the library default, 8).
+
+    Use ``with gate.member():`` around a member thread's work, and attach the
+    gate to its model (``Model.batch_gate = gate``)."""
+
+    def __init__(self, device=None, cluster=0):
+        self.device = torch.device(device if device is not None else "cuda")
+        self.cluster = int(cluster)
+        self.cv = threading.Condition()
+        self.members = 0
+        self.running = 0
+        self.pending = []
+        self.streams = {}
+        self.ws = {}
+        # statistics: launches per kind and models per launch
+        self.launches = {k: 0 for k in KINDS}
+        self.solves = {k: 0 for k in KINDS}
+
+    # ------------------------------------------------------- membership
+    def join(self):
+        with self.cv:
+            self.members += 1
+            self.running += 1
+
+    def leave(self):
+        with self.cv:
+            self.members -= 1
+            self.running -= 1
+            self._maybe_flush()
+
+    @contextmanager
+    def member(self):
+        self.join()
+        try:
+            yield self
+        finally:
+            self.leave()
+
+    # ----------------------------------------------------------- solves
+    def submit(self, name, grid, args, status, ws, ws_bytes, cycle):
+        """Called by a member thread in place of tse_<name>_dc; returns once
+        the solve is queued behind this thread's current stream."""
+        if name not in KINDS:
+            raise ValueError("no batched form of %s" % name)
+        req = _Request(name, grid, args, status, ws, ws_bytes,
+                       torch.cuda.current_stream(self.device), int(cycle))
+        with self.cv:
+            if self.members < 1:
+                raise RuntimeError("BatchGate.submit from a thread that has not joined the gate")
+            self.pending.append(req)
+            self.running -= 1
+            self._maybe_flush()
+            while not req.done:
+                self.cv.wait()
+        if req.error is not None:
+            raise req.error
+
+    def _maybe_flush(self):
+        # caller holds self.cv
+        if self.running > 0 or not self.pending:
+            return
+        reqs, self.pending = self.pending, []
+        try:
+            self._launch(reqs)
+        except Exception as e:   # every waiting member sees the failure
+            for r in reqs:
+                r.error = e
+        for r in reqs:
+            r.done = True
+        self.running += len(reqs)
+        self.cv.notify_all()
+
+    def _stream(self, key):
+        s = self.streams.get(key)
+        if s is None:
+            s = self.streams[key] = torch.cuda.Stream(device=self.device)
+        return s
+
+    def _workspace(self, key, n, stream):
+        need = int(N.lib().tse_batch_workspace_bytes(n))
+        t = self.ws.get(key)
+        if t is None or t.numel() < need:
+            with torch.cuda.stream(stream):
+                t = self.ws[key] = torch.empty(need, dtype=torch.uint8, device=self.device)
+        return t
+
+    def _launch(self, reqs):
+        L = N.lib()
+        groups = {}
+        for r in reqs:
+            groups.setdefault((r.name, r.cycle), []).append(r)
+        with torch.cuda.device(self.device):
+            for (name, cycle), rs in groups.items():
+                bs = self._stream((name, cycle))
+                seen = set()
+                for r in rs:
+                    if r.stream.cuda_stream not in seen:
+                        seen.add(r.stream.cuda_stream)
+                        bs.wait_stream(r.stream)
+                ws = self._workspace((name, cycle), len(rs), bs)
+                Item = N.BATCH_ITEM[name]
+                items = (Item * len(rs))(*[Item(ct.pointer(r.grid), ct.pointer(r.args),
+                                                ct.c_void_p(r.status.data_ptr()),
+                                                ct.c_void_p(r.ws.data_ptr()), r.ws_bytes)
+                                           for r in rs])
+                opts = N.TseDcOptions(cycle, self.cluster, 0)
+                rc = getattr(L, "tse_%s_dc_batch" % name)(items, len(rs), ct.byref(opts),
+                                                          ct.c_void_p(ws.data_ptr()), ws.numel(),
+                                                          ct.c_void_p(bs.cuda_stream))
+                N.check(rc, "tse_%s_dc_batch" % name)
+                self.launches[name] += 1
+                self.solves[name] += len(rs)
+                for r in rs:
+                    r.stream.wait_stream(bs)
+
+    def stats(self):
+        return {"launches": dict(self.launches), "solves": dict(self.solves)}

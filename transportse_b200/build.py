@@ -31,6 +31,7 @@ SOURCES = {
     "tse_flow.cu": ["--fmad=false"],
     "tse_capi.cu": ["--fmad=false"],
     "tse_dc.cu": [],
+    "tse_batch.cu": [],
 }
 
 

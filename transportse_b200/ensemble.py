@@ -4,12 +4,25 @@ A parameter or permeability ensemble is a list of config modules of uneven
 grid sizes that share nothing.  ``Ensemble`` advances them concurrently: up
 to ``concurrency`` models are resident at once, each driven by its own host
 thread on its own CUDA stream through the full time-step driver
-(``driver.Simulation``: SIA loop, pressure, fluxes, transport, EOS).  The
-cooperative sweep kernels of the concurrent solves share the SMs, each capped
-to its share of the co-resident blocks, so small models fill the GPU together
-instead of each paying a whole-GPU barrier per half-sweep.  Models are
-admitted as earlier ones finish and their device memory is returned, under an
-HBM budget.
+(``driver.Simulation``: SIA loop, pressure, fluxes, transport, EOS), so every
+model progresses at its own pace.  Models are admitted as earlier ones finish
+and their device memory is returned, under an HBM budget.
+
+How a model's mixed-precision solves run depends on its size:
+  * grids of up to ``cluster_cells`` cells: each solve is one launch of one
+    thread-block cluster (tse_compute_*_dc_batch with one item) -- no
+    device-wide barrier, no host round trip -- so many small models stream
+    side by side;
+  * larger grids: the cooperative whole-GPU sweeps, each capped to its share
+    of the co-resident blocks.
+With ``batched=True`` the threads instead meet at a ``BatchGate``
+(transportse_b200.batch), which runs each kind of solve of all waiting models
+as one launch in lock step; that suits ensembles of equal models, since a
+batch lasts as long as its slowest member.
+
+More than eight concurrent streams need CUDA_DEVICE_MAX_CONNECTIONS raised
+(e.g. to 32) before the process creates its CUDA context, or their launches
+serialise on the default eight hardware queues.
 
 The ctypes entry points release the GIL while they run, so the host threads
 overlap; every model's result is independent of which others run beside it
@@ -26,6 +39,7 @@ import numpy
 import torch
 
 from . import _native as N
+from .batch import BatchGate
 from .driver import Simulation
 
 # resident cooperative blocks per SM of the mixed-precision sweep kernel
@@ -105,13 +119,28 @@ def block_cap(device, concurrency):
     return max(8, (sms * SWEEP_BLOCKS_PER_SM) // max(1, concurrency))
 
 
-def run_model(config, steps, device, precision, max_blocks, dc_cycle=None, keep=("P", "C", "T")):
-    """Run one model on the calling thread's current stream; returns results."""
+def run_model(config, steps, device, precision, max_blocks, dc_cycle=None, keep=("P", "C", "T"),
+              gate=None, cluster_cells=0, cluster_size=0):
+    """Run one model on the calling thread's current stream; returns results.
+    With ``gate`` its mixed-precision solves are batched through it; else a
+    grid of at most ``cluster_cells`` cells solves in single-cluster launches
+    (``cluster_size`` CTAs) on this stream."""
     sim = Simulation(config, device=device, precision=precision)
     sim.M.max_blocks = int(max_blocks)
+    sim.M.cluster_cells = int(cluster_cells)
+    if cluster_size:
+        sim.M.cluster_size = int(cluster_size)
     if dc_cycle:
         sim.M.dc_cycle = int(dc_cycle)
-    sim.run(max_steps=steps)
+    if gate is not None:
+        with gate.member():
+            sim.M.batch_gate = gate
+            try:
+                sim.run(max_steps=steps)
+            finally:
+                sim.M.batch_gate = None
+    else:
+        sim.run(max_steps=steps)
     out = {k: sim.field(k) for k in keep}
     out["cell_updates"] = cell_updates(sim)
     out["steps"] = sim.n_tsteps
@@ -120,35 +149,66 @@ def run_model(config, steps, device, precision, max_blocks, dc_cycle=None, keep=
     return out
 
 
-def autotune(configs, device=None, precision="fp32dc", steps=1,
-             concurrency=(2, 4, 8), cycles=(64, 128, 256)):
-    """Pick the concurrency (models in flight, hence blocks per model) and the
-    correction-cycle length that give the highest cell-update rate on a
-    sample of the ensemble.  Returns {"concurrency", "dc_cycle", "rate",
-    "trials"}; the sample runs from the models' initial state each time."""
+def autotune(configs, device=None, precision="fp32dc", steps=1, concurrency=(2, 4, 8),
+             cycles=(128,), cluster_cells=(0,), batched=False, clusters=(8, 16)):
+    """Pick the launch shape that gives the highest cell-update rate on a
+    sample of the ensemble: unbatched, the concurrency (models in flight),
+    the largest grid solved by single-cluster launches and the
+    correction-cycle length; batched, the cluster size (CTAs per model) and
+    cycle length.  Returns the best parameter set with its "rate" and all
+    "trials"; the sample runs from the models' initial state each time."""
+    space = []
+    if batched:
+        for c in clusters:
+            for cyc in cycles:
+                space.append({"batched": True, "cluster": c, "dc_cycle": cyc})
+    else:
+        for k in concurrency:
+            for cc in cluster_cells:
+                for cyc in cycles:
+                    space.append({"batched": False, "concurrency": k, "cluster_cells": cc,
+                                  "dc_cycle": cyc})
     trials = []
     best = None
-    for k in concurrency:
-        for cyc in cycles:
-            _, st = Ensemble(configs, device=device, precision=precision, concurrency=k,
-                             dc_cycle=cyc).run(steps, keep=())
-            trials.append({"concurrency": k, "dc_cycle": cyc, "rate": st["cell_updates_per_s"]})
-            if best is None or st["cell_updates_per_s"] > best["rate"]:
-                best = dict(trials[-1])
+    for p in space:
+        _, st = Ensemble(configs, device=device, precision=precision, **p).run(steps, keep=())
+        trials.append(dict(p, rate=st["cell_updates_per_s"]))
+        if best is None or trials[-1]["rate"] > best["rate"]:
+            best = dict(trials[-1])
     best["trials"] = trials
     return best
 
 
+# grids up to this many cells take single-cluster solves by default
+CLUSTER_CELLS = 0
+
+
 class Ensemble:
-    def __init__(self, configs, device=None, precision="fp32dc", concurrency=4, hbm_budget=None,
-                 max_blocks=None, dc_cycle=None):
+    """``concurrency``: models in flight (None: 4, or every model when
+    batched).  ``batched``: solve in lock step through a BatchGate.
+    ``cluster``: CTAs per model in cluster launches (0: 16 alone, 8 batched).
+    ``cluster_cells``: largest grid (cells) solved by single-cluster launches
+    when not batched (None: CLUSTER_CELLS)."""
+
+    def __init__(self, configs, device=None, precision="fp32dc", concurrency=None, hbm_budget=None,
+                 max_blocks=None, dc_cycle=None, batched=False, cluster=0, cluster_cells=None):
         self.configs = list(configs)
         self.device = torch.device(device if device is not None else "cuda")
         self.precision = precision
-        self.concurrency = max(1, int(concurrency))
+        self.batched = bool(batched)
+        if self.batched and precision != "fp32dc":
+            raise ValueError("batched solves need precision='fp32dc'")
+        self.cluster_cells = CLUSTER_CELLS if cluster_cells is None else int(cluster_cells)
+        if precision != "fp32dc":
+            self.cluster_cells = 0
+        if concurrency is None:
+            concurrency = len(self.configs) if self.batched else 4
+        self.concurrency = max(1, min(int(concurrency), max(1, len(self.configs))))
         self.budget = HbmBudget(hbm_budget if hbm_budget is not None else default_budget(self.device))
         self.max_blocks = max_blocks if max_blocks else block_cap(self.device, self.concurrency)
         self.dc_cycle = dc_cycle
+        self.cluster = int(cluster)
+        self.gate = BatchGate(self.device, cluster=self.cluster) if self.batched else None
 
     def run(self, steps, keep=("P", "C", "T")):
         """Advance every model by ``steps`` time steps; returns (results, stats)."""
@@ -171,7 +231,8 @@ class Ensemble:
                 try:
                     with torch.cuda.device(self.device), torch.cuda.stream(stream):
                         results[i] = run_model(cfg, steps, self.device, self.precision,
-                                               self.max_blocks, self.dc_cycle, keep)
+                                               self.max_blocks, self.dc_cycle, keep, self.gate,
+                                               self.cluster_cells, self.cluster)
                         stream.synchronize()
                 except Exception as e:   # reported after all workers stop
                     errors.append((i, e))
@@ -191,4 +252,6 @@ class Ensemble:
         return results, {"wall_s": wall, "cell_updates": updates,
                          "cell_updates_per_s": updates / wall if wall > 0 else 0.0,
                          "models": len(results), "concurrency": self.concurrency,
-                         "max_blocks": self.max_blocks}
+                         "max_blocks": self.max_blocks, "batched": self.batched,
+                         "cluster_cells": self.cluster_cells,
+                         "batch": self.gate.stats() if self.gate is not None else None}

@@ -98,6 +98,18 @@ class Model:
         """Call tse_<name> or its mixed-precision form tse_<name>_dc."""
         L = N.lib()
         if self.precision == "fp32dc" and conv >= getattr(self, "dc_min_conv", self.DC_MIN_CONV):
+            gate = getattr(self, "batch_gate", None)
+            if gate is not None:
+                # batched with the other models' solves (transportse_b200.batch)
+                gate.submit(name, self.grid, args_struct, self.status, self.ws, self.ws_bytes,
+                            self.dc_cycle)
+                return
+            if self.n <= self.cluster_cells:
+                # small grid: the whole solve as one launch of one thread-block
+                # cluster, no device-wide barriers and no host round trips,
+                # leaving the rest of the GPU to other streams
+                self._solve_cluster(name, args_struct)
+                return
             opts = N.TseDcOptions(self.dc_cycle, getattr(self, "max_blocks", 0), int(self.timing))
             rc = getattr(L, "tse_%s_dc" % name)(ct.byref(self.grid), ct.byref(args_struct),
                                                 ct.byref(opts), self._p(self.status),
@@ -112,6 +124,25 @@ class Model:
                                            self._p(self.status), self._p(self.ws), self.ws_bytes,
                                            self._stream())
         N.check(rc, "tse_" + name)
+
+    # grids of up to this many cells solve in one cluster launch (0: never);
+    # cluster_size CTAs per cluster (0: library default)
+    cluster_cells = 0
+    cluster_size = 16
+
+    def _solve_cluster(self, name, args_struct):
+        L = N.lib()
+        bws = self.__dict__.get("_cluster_ws")
+        if bws is None:
+            bws = self._cluster_ws = torch.empty(int(L.tse_batch_workspace_bytes(1)),
+                                                 dtype=torch.uint8, device=self.device)
+        Item = N.BATCH_ITEM[name]
+        items = (Item * 1)(Item(ct.pointer(self.grid), ct.pointer(args_struct),
+                                self._p(self.status), self._p(self.ws), self.ws_bytes))
+        opts = N.TseDcOptions(self.dc_cycle, int(self.cluster_size), 0)
+        rc = getattr(L, "tse_%s_dc_batch" % name)(items, 1, ct.byref(opts), self._p(bws),
+                                                  bws.numel(), self._stream())
+        N.check(rc, "tse_%s_dc_batch" % name)
 
     # ----------------------------------------------------------- helpers
     def _t(self, a):

@@ -3,11 +3,14 @@
 ``Server`` admits requests (a config module and a number of time steps) as
 slots and device memory free up, keeps each admitted model's state resident
 on the GPU until its last step, and runs the admitted models concurrently,
-one host thread and CUDA stream per slot (the cooperative sweep kernels of
-concurrent solves each take a share of the SMs).  A request that arrives
-while others are running starts as soon as a slot is free and its state fits
-the HBM budget, so its sweeps overlap theirs on the device -- continuous
-batching at the granularity of solver launches.
+one host thread and CUDA stream per slot.  With ``batched`` (the default for
+the mixed-precision form) the slots' solves meet at a ``BatchGate``: each
+kind of solve of all admitted models runs as one launch, one thread-block
+cluster per model; otherwise the cooperative sweep kernels of concurrent
+solves each take a share of the SMs.  A request that arrives while others are
+running starts as soon as a slot is free and its state fits the HBM budget,
+and joins the next batch of solves -- continuous batching at the granularity
+of solver calls.
 
 ``replay(trace)`` plays a trace of (arrival time, config, steps) in real time
 and reports per-request latency (arrival to result), p50/p99 and the
@@ -22,6 +25,7 @@ import time
 import numpy
 import torch
 
+from .batch import BatchGate
 from .ensemble import HbmBudget, block_cap, default_budget, run_model, state_bytes
 
 
@@ -45,9 +49,13 @@ class Request:
 
 class Server:
     def __init__(self, device=None, slots=8, hbm_budget=None, precision="fp32dc", max_blocks=None,
-                 keep=("P", "C", "T")):
+                 keep=("P", "C", "T"), batched=None, cluster=0):
         self.device = torch.device(device if device is not None else "cuda")
         self.slots = max(1, int(slots))
+        self.batched = (precision == "fp32dc") if batched is None else bool(batched)
+        if self.batched and precision != "fp32dc":
+            raise ValueError("batched solves need precision='fp32dc'")
+        self.gate = BatchGate(self.device, cluster=cluster) if self.batched else None
         self.budget = HbmBudget(hbm_budget if hbm_budget is not None else default_budget(self.device))
         self.precision = precision
         self.max_blocks = max_blocks if max_blocks else block_cap(self.device, self.slots)
@@ -99,7 +107,7 @@ class Server:
                 req.start = self.now()
                 with torch.cuda.device(self.device), torch.cuda.stream(stream):
                     req.result = run_model(req.config, req.steps, self.device, self.precision,
-                                           self.max_blocks, keep=self.keep)
+                                           self.max_blocks, keep=self.keep, gate=self.gate)
                     stream.synchronize()
             except Exception as e:
                 req.error = e
@@ -138,7 +146,9 @@ class Server:
                       "p99_s": float(numpy.percentile(lat, 99)), "mean_s": float(lat.mean()),
                       "makespan_s": makespan, "cell_updates": updates,
                       "cell_updates_per_s": updates / makespan if makespan > 0 else 0.0,
-                      "slots": self.slots, "max_blocks": self.max_blocks}
+                      "slots": self.slots, "max_blocks": self.max_blocks,
+                      "batched": self.batched,
+                      "batch": self.gate.stats() if self.gate is not None else None}
 
 
 def poisson_trace(n, rate, seed, builder, steps, **kw):
