@@ -452,9 +452,12 @@ def kernel_only(a):
     M.dc_min_conv = 0.0   # P_conv = 0 below: keep the requested form
     P0 = S["P"].clone()
     peak, kind = measured_peak()
+    M.timing = a.kernel_only == "fp32dc"
     out = []
+    sweep = []
     for r in range(a.repeat + 1):
         S["P"].copy_(P0)
+        M.sweep_timed.clear()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
@@ -466,13 +469,24 @@ def kernel_only(a):
         torch.cuda.synchronize()
         if r:
             out.append((e0.elapsed_time(e1), res[5]))
+            if M.sweep_timed:
+                sweep.append((sum(x[3] for x in M.sweep_timed), sum(x[2] for x in M.sweep_timed)))
     active = int((S["BP"] == 0).sum().item())
     ms = statistics.median(x[0] for x in out)
     its = out[0][1]
     rate = its * active / (ms / 1e3)
     st = M.last_status
+    sw = None
+    if sweep:
+        # the sweep kernel alone (event-timed launches), without the solve's
+        # FP64 setup, residual and unpack passes
+        sms = statistics.median(x[0] for x in sweep)
+        sw = {"ms": sms, "us_per_iteration": 1e3 * sms / sweep[0][1],
+              "cell_updates_per_s": sweep[0][1] * active / (sms / 1e3),
+              "frac_of_peak": sweep[0][1] * active / (sms / 1e3) * ALG_BYTES["fp32dc"] / 1e9 / peak}
     print(json.dumps({"kernel_only": a.kernel_only, "shape": list(shape), "iterations": its,
                       "residual_cycles": int(st.cycles), "halvings": int(st.halvings),
+                      "sweep_kernel": sw,
                       "ms_per_launch": ms, "cell_updates_per_s": rate,
                       "alg_GBps": rate * ALG_BYTES[a.kernel_only] / 1e9,
                       "frac_of_peak": rate * ALG_BYTES[a.kernel_only] / 1e9 / peak,

@@ -17,8 +17,10 @@
 // d's rounding and the iteration counts track the FP64 form's.
 //
 // Kernels: the FP32 sweeps run in one cooperative kernel that iterates until
-// an event (converged, cycle end, dt halving, stop); it needs 48 registers,
-// so 5 blocks fit per SM.  The FP64 residual, the x += d update and the dt
+// an event (converged, cycle end, dt halving, stop): dc_sweep_tma_kernel,
+// which stages each chunk's data in shared memory with bulk asynchronous
+// copies, or, where its stages do not fit, dc_sweep_kernel (48 registers,
+// 5 blocks per SM, plain loads).  The FP64 residual, the x += d update and the dt
 // halving (reset + new R terms) are separate, ordinary kernels, so their
 // register appetite does not limit the sweeps' occupancy.  The host reads one
 // small state record per correction cycle.
@@ -248,6 +250,369 @@ __global__ void __launch_bounds__(kSweepBlock, kSweepMinBlocks) dc_sweep_kernel(
     }
 }
 
+// ------------------------------------------------ FP32 sweeps, TMA-staged
+// The same iterations as dc_sweep_kernel, with the memory side rebuilt for
+// bytes in flight: the cells of a colour are cut into chunks of kTmaChunk,
+// block b takes chunks b, b + G, ...; for each chunk one thread issues bulk
+// asynchronous copies (cp.async.bulk, completion counted on an mbarrier) of
+// everything the chunk's relaxations read -- the 24-byte coefficient records,
+// r', the flag bytes, the old correction and three windows of the other
+// colour's correction (x+, x-, and one covering y+-, z+-) -- into one of
+// kTmaStages shared-memory stages.  The block computes chunk i from its stage
+// while the following chunks are in flight, so each SM keeps ~140 KB of reads
+// outstanding with no registers held for them.  The per-cell arithmetic is
+// relax()'s, operation for operation, so the corrections are identical to
+// dc_sweep_kernel's; only the grouping of the check sums differs.
+#ifndef TSE_TMA_CHUNK
+#define TSE_TMA_CHUNK 512
+#endif
+#ifndef TSE_TMA_STAGES
+#define TSE_TMA_STAGES 3
+#endif
+#ifndef TSE_TMA_MINB
+#define TSE_TMA_MINB 2
+#endif
+constexpr int kTmaChunk = TSE_TMA_CHUNK;
+constexpr int kTmaStages = TSE_TMA_STAGES;
+constexpr int kTmaBlock = 256;
+static_assert(kTmaChunk % kTmaBlock == 0 && kTmaChunk % 32 == 0, "chunk: whole trips, 16-byte copies");
+static_assert(kTmaChunk <= kDcMaxChunk, "windows must stay inside the correction margins");
+
+// byte offsets of one stage's arrays (all multiples of 16)
+struct TmaStage {
+    int rec, rp, msk, dw, wz, wxp, wxm, bytes;
+    int lz, lx;   // window lengths in floats
+};
+
+__host__ __device__ inline TmaStage tma_stage(int H) {
+    TmaStage t;
+    const int C = kTmaChunk;
+    t.rec = 0;
+    t.rp = 24 * C;
+    t.msk = t.rp + 4 * C;
+    t.dw = t.msk + C;
+    t.wz = t.dw + 4 * C;
+    // [m0 - H - 1, m0 + C + H] from a start rounded down by up to 3 floats
+    t.lz = (C + 2 * H + 5 + 3) & ~3;
+    // [m0 +- SX, m0 +- SX + C) from a start rounded down by up to 3 floats
+    t.lx = C + 4;
+    t.wxp = t.wz + 4 * t.lz;
+    t.wxm = t.wxp + 4 * t.lx;
+    t.bytes = (t.wxm + 4 * t.lx + 127) & ~127;
+    return t;
+}
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+// the stage's single arrival, adding `bytes` to its transaction count
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+// adds `bytes` to the transaction count without arriving
+__device__ __forceinline__ void mbar_add_tx(uint64_t* bar, unsigned bytes) {
+    asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+// bulk copy global -> this CTA's shared memory; 16-byte aligned, size % 16 == 0
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+// orders this thread's generic-proxy global accesses with async-proxy copies
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async;" ::: "memory"); }
+
+// bounded wait for a stage; false after kBarrierTimeoutNs
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = globaltimer();
+    unsigned spins = 0;
+    while (!mbar_try_wait(bar, parity)) {
+        if ((++spins & 63u) == 0u && globaltimer() - t0 > kBarrierTimeoutNs) return false;
+    }
+    return true;
+}
+
+// Chunk q of the colour being swept, in two parts.  The first part (records,
+// r', flags, the chunk's own old correction) depends on nothing another block
+// writes during the launch -- the old correction of a chunk is written only
+// by the block that owns the chunk -- so it may be issued before the grid
+// barrier that ends the previous phase; it adds its bytes to the stage's
+// transaction count without arriving.  The second part (the three windows of
+// the other colour, which other blocks have just written) is issued after the
+// barrier and carries the stage's single arrival.
+__device__ __forceinline__ void tma_issue_own(const DcCtl& c, const TmaStage& T, unsigned char* stage,
+                                              uint64_t* bar, const float* Kc, const float* dw,
+                                              const uint8_t* msk, long long q) {
+    const long long C = kTmaChunk, N = c.Ncal;
+    const long long m0 = q * C;
+    // cells [m0, m0 + cnt) lie inside the Ncal-padded arrays; cnt % 32 == 0
+    const long long cnt = (N - m0) < C ? (N - m0) : C;
+    const unsigned b_rec = (unsigned)(24 * cnt), b_rp = (unsigned)(4 * cnt), b_msk = (unsigned)cnt,
+                   b_dw = (unsigned)(4 * cnt);
+    mbar_add_tx(bar, b_rec + b_rp + b_msk + b_dw);
+    bulk_g2s(stage + T.rec, Kc + 6 * m0, b_rec, bar);
+    bulk_g2s(stage + T.rp, Kc + 6 * N + m0, b_rp, bar);
+    bulk_g2s(stage + T.msk, msk + m0, b_msk, bar);
+    bulk_g2s(stage + T.dw, dw + m0, b_dw, bar);
+}
+
+__device__ __forceinline__ void tma_issue_windows(const DcCtl& c, const TmaStage& T, unsigned char* stage,
+                                                  uint64_t* bar, const float* dq, long long q) {
+    const long long C = kTmaChunk, SX = c.L.SX;
+    const int H = c.L.H;
+    const long long m0 = q * C;
+    const long long zs = (m0 - H - 1) & ~3LL;
+    const long long xps = (m0 + SX) & ~3LL;
+    const long long xms = (m0 - SX) & ~3LL;
+    const unsigned b_z = (unsigned)(4 * T.lz), b_x = (unsigned)(4 * T.lx);
+    mbar_expect_tx(bar, b_z + 2 * b_x);
+    bulk_g2s(stage + T.wz, dq + zs, b_z, bar);
+    bulk_g2s(stage + T.wxp, dq + xps, b_x, bar);
+    bulk_g2s(stage + T.wxm, dq + xms, b_x, bar);
+}
+
+__global__ void __launch_bounds__(kTmaBlock, TSE_TMA_MINB) dc_sweep_tma_kernel(DcCtl c, TmaStage T) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) uint64_t mbar[kTmaStages];
+    __shared__ double sh[kTmaBlock / 32];
+    __shared__ int s_ok;
+    const unsigned nb = gridDim.x, b = blockIdx.x;
+    const int tid = threadIdx.x;
+    const long long Nc = c.L.Nc, SX = c.L.SX, C = kTmaChunk;
+    const int H = c.L.H;
+    const long long nch = (Nc + C - 1) / C;
+    const long long mine = nch > (long long)b ? (nch - 1 - b) / nb + 1 : 0;   // chunks of this block
+    const long long pro = mine < kTmaStages ? mine : kTmaStages;             // primed per phase
+    const bool leader = (b == 0 && tid == 0);
+    const float sor = c.sor;
+    DcState* st = c.st;
+    double t = st->t, dt = st->dt, diff = 1e100;
+    const double x2 = st->x2;
+    int num_it = st->num_it, num_sub_it = st->num_sub_it, checkno = st->checkno;
+    int event = EV_CYCLE_END;
+    bool halved = false;
+
+    unsigned uses = 0;   // chunks this block has consumed, over all colour phases
+    if (tid == 0) {
+        for (int s = 0; s < kTmaStages; ++s) mbar_init(&mbar[s], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_ok = 1;
+        // the first phase's own parts (the launch boundary orders them)
+        for (long long i = 0; i < pro; ++i) {
+            const unsigned s = (unsigned)i % kTmaStages;
+            tma_issue_own(c, T, smem + (size_t)s * T.bytes, &mbar[s], c.K[0], c.D[0], c.mask[0],
+                          b + i * nb);
+        }
+    }
+    __syncthreads();
+    // thread 0, after a failed wait: the uses whose copies may still be in flight
+    unsigned drain_lo = 0, drain_hi = 0;
+    bool primed = true;   // own parts of the next phase's first chunks are in flight
+
+    for (int inner = 0; inner < c.cycle; ++inner) {
+        num_it += 1;
+        num_sub_it += 1;
+        const bool check = c.pressure_schedule ? (num_it < 50 || num_it % 10 == 0) : true;
+        if (check) checkno += 1;
+        float d2 = 0.0f, dd = 0.0f;
+        bool ok = true;
+        for (int col = 0; col < 2 && ok; ++col) {
+            const float* Kc = c.K[col];
+            float* dw = c.D[col];
+            const float* dq = c.D[1 - col];
+            const uint8_t* msk = c.mask[col];
+            if (tid == 0) {
+                // the other colour was written (generic stores) before the
+                // grid barrier; the copies below read it through the async proxy
+                fence_proxy_async();
+                for (long long i = 0; i < pro; ++i) {
+                    const unsigned s = (uses + (unsigned)i) % kTmaStages;
+                    tma_issue_windows(c, T, smem + (size_t)s * T.bytes, &mbar[s], dq, b + i * nb);
+                }
+            }
+            primed = false;
+            for (long long i = 0; i < mine; ++i) {
+                const unsigned u = uses + (unsigned)i;
+                const unsigned s = u % kTmaStages;
+                unsigned char* stg = smem + (size_t)s * T.bytes;
+                if (tid == 0 && !mbar_wait_bounded(&mbar[s], (u / kTmaStages) & 1u)) {
+                    s_ok = 0;
+                    drain_lo = u;
+                    drain_hi = uses + (unsigned)(mine < i + kTmaStages ? mine : i + kTmaStages);
+                }
+                __syncthreads();
+                if (!s_ok) { ok = false; break; }   // block-uniform
+                // each thread observes the completed phase itself (acquire)
+                mbar_try_wait(&mbar[s], (u / kTmaStages) & 1u);
+                const long long q = b + i * nb;
+                const long long m0 = q * C;
+                const long long zs = (m0 - H - 1) & ~3LL;
+                const long long xps = (m0 + SX) & ~3LL;
+                const long long xms = (m0 - SX) & ~3LL;
+                const float2* rec = reinterpret_cast<const float2*>(stg + T.rec);
+                const float* rp = reinterpret_cast<const float*>(stg + T.rp);
+                const uint8_t* fl = stg + T.msk;
+                const float* dwo = reinterpret_cast<const float*>(stg + T.dw);
+                const float* wz = reinterpret_cast<const float*>(stg + T.wz);
+                const float* wxp = reinterpret_cast<const float*>(stg + T.wxp);
+                const float* wxm = reinterpret_cast<const float*>(stg + T.wxm);
+#pragma unroll
+                for (int r = 0; r < kTmaChunk / kTmaBlock; ++r) {
+                    const int l = tid + r * kTmaBlock;
+                    const long long m = m0 + l;
+                    if (m < Nc) {
+                        const float2 k01 = rec[3 * l], k23 = rec[3 * l + 1], k45 = rec[3 * l + 2];
+                        const bool odd = (fl[l] & F_KODD) != 0;
+                        const float old = dwo[l];
+                        const int iz = (int)(m - zs);
+                        const float z0 = wz[iz - 1], z1 = wz[iz], z2 = wz[iz + 1];
+                        float acc = rp[l];
+                        acc = fmaf(k01.x, wxp[m + SX - xps], acc);
+                        acc = fmaf(k01.y, wxm[m - SX - xms], acc);
+                        acc = fmaf(k23.x, wz[iz + H], acc);
+                        acc = fmaf(k23.y, wz[iz - H], acc);
+                        acc = fmaf(k45.x, odd ? z2 : z1, acc);
+                        acc = fmaf(k45.y, odd ? z1 : z0, acc);
+                        const float na = fmaf(sor, acc - old, old);
+                        dw[m] = na;
+                        const float ch = na - old;
+                        d2 = fmaf(ch, ch, d2);
+                        dd = fmaf(na, na, dd);
+                    }
+                }
+                __syncthreads();   // stage s is free again
+                if (tid == 0 && i + kTmaStages < mine) {
+                    const long long qn = b + (i + kTmaStages) * nb;
+                    tma_issue_own(c, T, stg, &mbar[s], Kc, dw, msk, qn);
+                    tma_issue_windows(c, T, stg, &mbar[s], dq, qn);
+                }
+            }
+            if (!ok) break;
+            uses += (unsigned)mine;
+            // this phase's stores are read by the next phase's copies
+            fence_proxy_async();
+            // own parts of the next phase's first chunks go out before the
+            // barrier (after the last iteration's second phase they are
+            // unused and drained at exit)
+            if (tid == 0) {
+                const int nc = 1 - col;
+                for (long long i = 0; i < pro; ++i) {
+                    const unsigned s = (uses + (unsigned)i) % kTmaStages;
+                    tma_issue_own(c, T, smem + (size_t)s * T.bytes, &mbar[s], c.K[nc], c.D[nc],
+                                  c.mask[nc], b + i * nb);
+                }
+            }
+            primed = true;
+            if (col == 1 && check) {
+                const double b1 = block_sum<kTmaBlock>((double)d2, sh);
+                const double b3 = block_sum<kTmaBlock>((double)dd, sh);
+                if (tid == 0) {
+                    c.partials[4 * b + 2 * (checkno & 1)] = b1;
+                    c.partials[4 * b + 2 * (checkno & 1) + 1] = b3;
+                }
+            }
+            ok = grid_sync(c.bar, nb);
+        }
+        if (!ok) { event = EV_ERROR; break; }
+        diff = 1e100;
+        bool refresh = false;
+        if (check) {
+            double s1 = 0.0, s3 = 0.0;
+            for (unsigned q = tid; q < nb; q += blockDim.x) {
+                s1 = s1 + __ldcg(c.partials + 4 * q + 2 * (checkno & 1));
+                s3 = s3 + __ldcg(c.partials + 4 * q + 2 * (checkno & 1) + 1);
+            }
+            s1 = block_sum<kTmaBlock>(s1, sh);
+            s3 = block_sum<kTmaBlock>(s3, sh);
+            if (tid == 0) {
+                sh[0] = s1;
+                sh[1] = s3;
+            }
+            __syncthreads();
+            s1 = sh[0];
+            s3 = sh[1];
+            __syncthreads();
+            const double l2 = sqrt(s1) / sqrt(x2 + 1e-200);
+            diff = (l2 != l2) ? 1.0 : l2;
+            refresh = sqrt(s1) < kRefresh * sqrt(s3);
+        }
+        if (diff < c.conv || c.stop_on_first) {
+            t += dt;
+            if (num_sub_it < c.max_it / 2.0) dt = pymin(dt * c.inc_it, c.max_dt);
+            event = EV_CONVERGED;
+            break;
+        }
+        if (num_sub_it >= c.max_it) {
+            if (leader && st->nev < 8) {
+                st->ev_it[st->nev] = num_it;
+                st->ev_dt[st->nev] = dt;
+                st->ev_diff[st->nev] = diff;
+            }
+            if (leader) st->nev += 1;
+            dt = dt / 2;
+            num_sub_it = 0;
+            halved = true;
+        }
+        if (dt <= c.min_dt) { event = halved ? EV_STOP_HALVED : EV_STOP; break; }
+        if (halved) { event = EV_HALVE; break; }
+        if (refresh) { event = EV_REFRESH; break; }
+    }
+    if (tid == 0) {
+        // let every copy this block issued land before its shared memory is
+        // released (bounded, like every wait here): primed stages get their
+        // missing arrival, so their phase completes once their bytes are in
+        if (event == EV_ERROR) atomicExch(&c.bar->error, 1);
+        for (unsigned u = drain_lo; u < drain_hi; ++u)
+            mbar_wait_bounded(&mbar[u % kTmaStages], (u / kTmaStages) & 1u);
+        if (primed)
+            for (long long i = 0; i < pro; ++i) {
+                const unsigned u = uses + (unsigned)i;
+                mbar_arrive(&mbar[u % kTmaStages]);
+                mbar_wait_bounded(&mbar[u % kTmaStages], (u / kTmaStages) & 1u);
+            }
+    }
+    if (leader) {
+        st->t = t;
+        st->dt = dt;
+        st->diff = diff;
+        st->num_it = num_it;
+        st->num_sub_it = num_sub_it;
+        st->checkno = checkno;
+        st->event = event;
+        if (halved) st->halvings += 1;
+        if (event == EV_CONVERGED) st->converged = 1;
+    }
+}
+
 // copy the final state into the caller's status record
 __global__ void dc_status_kernel(const DcState* st, TseSolveStatus* s) {
     s->t = st->t;
@@ -293,6 +658,37 @@ static int sweep_blocks(long long Nc, int cap) {
     return (int)nb;
 }
 
+#ifndef TSE_SWEEP_TMA
+#define TSE_SWEEP_TMA 1   // 1: TMA-staged sweeps where the stages fit in shared memory
+#endif
+constexpr size_t kTmaMaxSmem = 200 * 1024;
+
+// blocks of the staged sweep: as many as fit (dynamic shared memory
+// included), at most one per chunk of a colour; 0 when the stages for this
+// grid's windows do not fit (the plain sweep kernel runs instead)
+static int tma_blocks(long long Nc, int cap, size_t smem) {
+    if (!TSE_SWEEP_TMA || smem > kTmaMaxSmem) return 0;
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    // the same ceiling for every grid, so concurrent callers never lower it
+    // below another's launch
+    if (cudaFuncSetAttribute(dc_sweep_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kTmaMaxSmem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dc_sweep_tma_kernel, kTmaBlock, smem) !=
+            cudaSuccess ||
+        per_sm < 1) {
+        cudaGetLastError();
+        return 0;
+    }
+    long long nb = (long long)sms * per_sm;
+    const long long nch = (Nc + kTmaChunk - 1) / kTmaChunk;
+    if (nb > nch) nb = nch;
+    if (nb > kMaxBlocks / 2) nb = kMaxBlocks / 2;
+    if (cap > 0 && nb > cap) nb = cap;
+    return nb < 1 ? 1 : (int)nb;
+}
+
 template <class Form>
 static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, double min_dt,
                   double conv, int max_it, int pressure_schedule, int stop_on_first,
@@ -324,7 +720,10 @@ static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, 
         return TSE_ERR_LAUNCH;
     const long long cells2 = 2 * S.L.Nc;
     const unsigned gcells = (unsigned)((cells2 + kBlock - 1) / kBlock);
-    const int nb = sweep_blocks(S.L.Nc, cap);
+    const TmaStage T = tma_stage(S.L.H);
+    const size_t tma_smem = (size_t)kTmaStages * T.bytes;
+    const int nb_tma = tma_blocks(S.L.Nc, cap, tma_smem);
+    const int nb = nb_tma > 0 ? nb_tma : sweep_blocks(S.L.Nc, cap);
     c.chunk = (S.L.Nc + nb - 1) / nb;
     c.R = neighbour_radius(S.L.SX, c.chunk, (unsigned)nb);
     dc_scale_kernel<<<gcells, kBlock, 0, stream>>>(S.F, c);
@@ -345,15 +744,23 @@ static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, 
         dc_residual_kernel<<<rb, kBlock, 0, stream>>>(S.F, c);
         dc_x2_kernel<<<1, kBlock, 0, stream>>>(c, (int)rb);
         void* args[] = {(void*)&c};
+        void* targs[] = {(void*)&c, (void*)&T};
         if (TSE_SWEEP_CHUNKED &&
             cudaMemsetAsync(c.prog, 0, (size_t)nb * sizeof(unsigned), stream) != cudaSuccess) {
             rc = TSE_ERR_LAUNCH;
             break;
         }
         if (timing) cudaEventRecord(ev0, stream);
-        if (cudaGetLastError() != cudaSuccess ||
-            cudaLaunchCooperativeKernel((const void*)dc_sweep_kernel, dim3(nb), dim3(kSweepBlock), args,
-                                        0, stream) != cudaSuccess) {
+        if (cudaGetLastError() != cudaSuccess) {
+            rc = TSE_ERR_LAUNCH;
+            break;
+        }
+        const cudaError_t le =
+            nb_tma > 0 ? cudaLaunchCooperativeKernel((const void*)dc_sweep_tma_kernel, dim3(nb),
+                                                     dim3(kTmaBlock), targs, tma_smem, stream)
+                       : cudaLaunchCooperativeKernel((const void*)dc_sweep_kernel, dim3(nb),
+                                                     dim3(kSweepBlock), args, 0, stream);
+        if (le != cudaSuccess) {
             rc = TSE_ERR_LAUNCH;
             break;
         }

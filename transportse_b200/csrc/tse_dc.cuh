@@ -109,8 +109,13 @@ __device__ __forceinline__ float relax(const Cell& a, const float* dq, long long
 
 // FP32 arrays: per colour 7 * Ncal floats (records + r'), then the
 // correction with margins of G >= SX + 1, then the state record and the
-// PhaseSync counters
-__host__ __device__ inline long long dc_margin(const Layout& L) { return ((L.SX + 1 + 63) / 64) * 64; }
+// PhaseSync counters.  The margins also hold the neighbour windows that the
+// staged sweep copies for a chunk of up to kDcMaxChunk cells at either end
+// (window starts rounded down to 16 bytes, lengths up to 8 floats longer).
+constexpr int kDcMaxChunk = 1024;
+__host__ __device__ inline long long dc_margin(const Layout& L) {
+    return ((L.SX + kDcMaxChunk + 16 + 63) / 64) * 64;
+}
 __host__ __device__ inline long long dc_delta_len(const Layout& L, long long Ncal) {
     return Ncal + 2 * dc_margin(L);
 }
