@@ -258,8 +258,8 @@ __global__ void __launch_bounds__(kSweepBlock, kSweepMinBlocks) dc_sweep_kernel(
 // everything the chunk's relaxations read -- the 24-byte coefficient records,
 // r', the flag bytes, the old correction and three windows of the other
 // colour's correction (x+, x-, and one covering y+-, z+-) -- into one of
-// kTmaStages shared-memory stages.  The block computes chunk i from its stage
-// while the following chunks are in flight, so each SM keeps ~140 KB of reads
+// kTmaStages shared-memory stages; the block computes from filled stages
+// while later chunks are in flight, so each SM keeps up to ~190 KB of reads
 // outstanding with no registers held for them.  The per-cell arithmetic is
 // relax()'s, operation for operation, so the corrections are identical to
 // dc_sweep_kernel's; only the grouping of the check sums differs.
@@ -267,15 +267,14 @@ __global__ void __launch_bounds__(kSweepBlock, kSweepMinBlocks) dc_sweep_kernel(
 #define TSE_TMA_CHUNK 512
 #endif
 #ifndef TSE_TMA_STAGES
-#define TSE_TMA_STAGES 3
+#define TSE_TMA_STAGES 4   // two stages in computation, the rest in flight
 #endif
 #ifndef TSE_TMA_MINB
 #define TSE_TMA_MINB 2
 #endif
 constexpr int kTmaChunk = TSE_TMA_CHUNK;
 constexpr int kTmaStages = TSE_TMA_STAGES;
-constexpr int kTmaBlock = 256;
-static_assert(kTmaChunk % kTmaBlock == 0 && kTmaChunk % 32 == 0, "chunk: whole trips, 16-byte copies");
+static_assert(kTmaChunk % 32 == 0, "chunk: 16-byte copies of every array");
 static_assert(kTmaChunk <= kDcMaxChunk, "windows must stay inside the correction margins");
 
 // byte offsets of one stage's arrays (all multiples of 16)
@@ -347,6 +346,46 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned by
         : "memory");
 }
 
+// L2 eviction priority.  Per iteration the coefficient records, r' and the
+// flags stream ~29 bytes a cell once (far more than L2 holds), while the two
+// correction arrays (8 bytes a cell) are reread by the next phase's windows:
+// the stream is marked evict-first and the corrections evict-last, so the
+// corrections stay in L2 instead of being pushed out by the stream.
+#ifndef TSE_TMA_HINTS
+#define TSE_TMA_HINTS 1
+#endif
+__device__ __forceinline__ uint64_t l2_evict_first() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint64_t l2_evict_last() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+__device__ __forceinline__ void bulk_g2s_hint(void* dst, const void* src, unsigned bytes, uint64_t* bar,
+                                              uint64_t policy) {
+#if TSE_TMA_HINTS
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+        " [%0], [%1], %2, [%3], %4;"
+        ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
+        : "memory");
+#else
+    bulk_g2s(dst, src, bytes, bar);
+#endif
+}
+
+__device__ __forceinline__ void st_hint(float* p, float v, uint64_t policy) {
+#if TSE_TMA_HINTS
+    asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(p), "f"(v), "l"(policy) : "memory");
+#else
+    *p = v;
+#endif
+}
+
 // orders this thread's generic-proxy global accesses with async-proxy copies
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async;" ::: "memory"); }
 
@@ -371,72 +410,104 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity
 // barrier and carries the stage's single arrival.
 __device__ __forceinline__ void tma_issue_own(const DcCtl& c, const TmaStage& T, unsigned char* stage,
                                               uint64_t* bar, const float* Kc, const float* dw,
-                                              const uint8_t* msk, long long q) {
-    const long long C = kTmaChunk, N = c.Ncal;
-    const long long m0 = q * C;
-    // cells [m0, m0 + cnt) lie inside the Ncal-padded arrays; cnt % 32 == 0
-    const long long cnt = (N - m0) < C ? (N - m0) : C;
+                                              const uint8_t* msk, long long m0, long long cnt) {
+    const long long N = c.Ncal;
     const unsigned b_rec = (unsigned)(24 * cnt), b_rp = (unsigned)(4 * cnt), b_msk = (unsigned)cnt,
                    b_dw = (unsigned)(4 * cnt);
+    const uint64_t first = l2_evict_first(), last = l2_evict_last();
     mbar_add_tx(bar, b_rec + b_rp + b_msk + b_dw);
-    bulk_g2s(stage + T.rec, Kc + 6 * m0, b_rec, bar);
-    bulk_g2s(stage + T.rp, Kc + 6 * N + m0, b_rp, bar);
-    bulk_g2s(stage + T.msk, msk + m0, b_msk, bar);
-    bulk_g2s(stage + T.dw, dw + m0, b_dw, bar);
+    bulk_g2s_hint(stage + T.rec, Kc + 6 * m0, b_rec, bar, first);
+    bulk_g2s_hint(stage + T.rp, Kc + 6 * N + m0, b_rp, bar, first);
+    bulk_g2s_hint(stage + T.msk, msk + m0, b_msk, bar, first);
+    bulk_g2s_hint(stage + T.dw, dw + m0, b_dw, bar, last);
+    (void)N;
 }
 
 __device__ __forceinline__ void tma_issue_windows(const DcCtl& c, const TmaStage& T, unsigned char* stage,
-                                                  uint64_t* bar, const float* dq, long long q) {
-    const long long C = kTmaChunk, SX = c.L.SX;
+                                                  uint64_t* bar, const float* dq, long long m0) {
+    const long long SX = c.L.SX;
     const int H = c.L.H;
-    const long long m0 = q * C;
     const long long zs = (m0 - H - 1) & ~3LL;
     const long long xps = (m0 + SX) & ~3LL;
     const long long xms = (m0 - SX) & ~3LL;
     const unsigned b_z = (unsigned)(4 * T.lz), b_x = (unsigned)(4 * T.lx);
+    const uint64_t last = l2_evict_last();
     mbar_expect_tx(bar, b_z + 2 * b_x);
-    bulk_g2s(stage + T.wz, dq + zs, b_z, bar);
-    bulk_g2s(stage + T.wxp, dq + xps, b_x, bar);
-    bulk_g2s(stage + T.wxm, dq + xms, b_x, bar);
+    bulk_g2s_hint(stage + T.wz, dq + zs, b_z, bar, last);
+    bulk_g2s_hint(stage + T.wxp, dq + xps, b_x, bar, last);
+    bulk_g2s_hint(stage + T.wxm, dq + xms, b_x, bar, last);
 }
 
-__global__ void __launch_bounds__(kTmaBlock, TSE_TMA_MINB) dc_sweep_tma_kernel(DcCtl c, TmaStage T) {
+// Roles: warps 0-7 consume, in two groups of four warps; group g computes the
+// block's chunks i = g, g + 2, ..., so two chunks are in computation at once
+// and neither waits for the other.  Warp 8 produces: its lane 0 issues the
+// copies of chunk i into stage i % kTmaStages as soon as the consumers of
+// chunk i - kTmaStages have released that stage (`empty` barrier, one arrival
+// per consumer warp).  Consumers wait on the stage's `full` barrier (the
+// copies' byte count).  Only the colour phases end in block- and grid-wide
+// barriers.  Every wait is bounded; a wait that runs out raises a block flag
+// that ends every other wait of the block, and the kernel leaves with
+// EV_ERROR after the copies still in flight have landed (again bounded).
+constexpr int kTmaConsumers = 256;                    // 8 warps, two groups of 4
+constexpr int kTmaGroup = kTmaConsumers / 2;
+constexpr int kTmaThreads = kTmaConsumers + 32;       // + one producer warp
+constexpr int kTmaCellsPerThread = kTmaChunk / kTmaGroup;
+static_assert(kTmaChunk % kTmaGroup == 0, "whole cells per consumer thread");
+
+// wait for a phase of `bar`; gives up (false) when the block's error flag is
+// raised or after kBarrierTimeoutNs, raising the flag
+__device__ __forceinline__ bool mbar_wait_flag(uint64_t* bar, unsigned parity, volatile int* err) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const uint64_t t0 = globaltimer();
+    unsigned spins = 0;
+    while (!mbar_try_wait(bar, parity)) {
+        if (*err) return false;
+        if ((++spins & 63u) == 0u && globaltimer() - t0 > kBarrierTimeoutNs) {
+            *err = 1;
+            return false;
+        }
+    }
+    return true;
+}
+
+__global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) dc_sweep_tma_kernel(DcCtl c, TmaStage T) {
     extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ __align__(8) uint64_t mbar[kTmaStages];
-    __shared__ double sh[kTmaBlock / 32];
-    __shared__ int s_ok;
+    __shared__ __align__(8) uint64_t full[kTmaStages];
+    __shared__ __align__(8) uint64_t empty[kTmaStages];
+    __shared__ double sh[kTmaThreads / 32];
+    __shared__ int s_err;
     const unsigned nb = gridDim.x, b = blockIdx.x;
     const int tid = threadIdx.x;
-    const long long Nc = c.L.Nc, SX = c.L.SX, C = kTmaChunk;
+    const int warp = tid >> 5, lane = tid & 31;
+    const bool producer = warp == kTmaConsumers / 32;
+    const int group = warp >> 2;                        // consumers: 0 or 1
+    const int gt = tid & (kTmaGroup - 1);               // thread within its group
+    const long long Nc = c.L.Nc, N = c.Ncal, SX = c.L.SX, C = kTmaChunk;
     const int H = c.L.H;
     const long long nch = (Nc + C - 1) / C;
     const long long mine = nch > (long long)b ? (nch - 1 - b) / nb + 1 : 0;   // chunks of this block
-    const long long pro = mine < kTmaStages ? mine : kTmaStages;             // primed per phase
     const bool leader = (b == 0 && tid == 0);
     const float sor = c.sor;
+    const uint64_t keep = l2_evict_last();
     DcState* st = c.st;
     double t = st->t, dt = st->dt, diff = 1e100;
     const double x2 = st->x2;
     int num_it = st->num_it, num_sub_it = st->num_sub_it, checkno = st->checkno;
     int event = EV_CYCLE_END;
     bool halved = false;
+    volatile int* err = &s_err;
 
-    unsigned uses = 0;   // chunks this block has consumed, over all colour phases
     if (tid == 0) {
-        for (int s = 0; s < kTmaStages; ++s) mbar_init(&mbar[s], 1);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        s_ok = 1;
-        // the first phase's own parts (the launch boundary orders them)
-        for (long long i = 0; i < pro; ++i) {
-            const unsigned s = (unsigned)i % kTmaStages;
-            tma_issue_own(c, T, smem + (size_t)s * T.bytes, &mbar[s], c.K[0], c.D[0], c.mask[0],
-                          b + i * nb);
+        for (int s = 0; s < kTmaStages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], kTmaConsumers / 64);   // one arrival per warp of a group
         }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_err = 0;
     }
     __syncthreads();
-    // thread 0, after a failed wait: the uses whose copies may still be in flight
-    unsigned drain_lo = 0, drain_hi = 0;
-    bool primed = true;   // own parts of the next phase's first chunks are in flight
+    unsigned uses = 0;      // chunks this block has consumed, over all colour phases
+    unsigned issued = 0;    // producer: chunks issued, over all colour phases
 
     for (int inner = 0; inner < c.cycle; ++inner) {
         num_it += 1;
@@ -450,91 +521,80 @@ __global__ void __launch_bounds__(kTmaBlock, TSE_TMA_MINB) dc_sweep_tma_kernel(D
             float* dw = c.D[col];
             const float* dq = c.D[1 - col];
             const uint8_t* msk = c.mask[col];
-            if (tid == 0) {
-                // the other colour was written (generic stores) before the
-                // grid barrier; the copies below read it through the async proxy
-                fence_proxy_async();
-                for (long long i = 0; i < pro; ++i) {
-                    const unsigned s = (uses + (unsigned)i) % kTmaStages;
-                    tma_issue_windows(c, T, smem + (size_t)s * T.bytes, &mbar[s], dq, b + i * nb);
-                }
-            }
-            primed = false;
-            for (long long i = 0; i < mine; ++i) {
-                const unsigned u = uses + (unsigned)i;
-                const unsigned s = u % kTmaStages;
-                unsigned char* stg = smem + (size_t)s * T.bytes;
-                if (tid == 0 && !mbar_wait_bounded(&mbar[s], (u / kTmaStages) & 1u)) {
-                    s_ok = 0;
-                    drain_lo = u;
-                    drain_hi = uses + (unsigned)(mine < i + kTmaStages ? mine : i + kTmaStages);
-                }
-                __syncthreads();
-                if (!s_ok) { ok = false; break; }   // block-uniform
-                // each thread observes the completed phase itself (acquire)
-                mbar_try_wait(&mbar[s], (u / kTmaStages) & 1u);
-                const long long q = b + i * nb;
-                const long long m0 = q * C;
-                const long long zs = (m0 - H - 1) & ~3LL;
-                const long long xps = (m0 + SX) & ~3LL;
-                const long long xms = (m0 - SX) & ~3LL;
-                const float2* rec = reinterpret_cast<const float2*>(stg + T.rec);
-                const float* rp = reinterpret_cast<const float*>(stg + T.rp);
-                const uint8_t* fl = stg + T.msk;
-                const float* dwo = reinterpret_cast<const float*>(stg + T.dw);
-                const float* wz = reinterpret_cast<const float*>(stg + T.wz);
-                const float* wxp = reinterpret_cast<const float*>(stg + T.wxp);
-                const float* wxm = reinterpret_cast<const float*>(stg + T.wxm);
-#pragma unroll
-                for (int r = 0; r < kTmaChunk / kTmaBlock; ++r) {
-                    const int l = tid + r * kTmaBlock;
-                    const long long m = m0 + l;
-                    if (m < Nc) {
-                        const float2 k01 = rec[3 * l], k23 = rec[3 * l + 1], k45 = rec[3 * l + 2];
-                        const bool odd = (fl[l] & F_KODD) != 0;
-                        const float old = dwo[l];
-                        const int iz = (int)(m - zs);
-                        const float z0 = wz[iz - 1], z1 = wz[iz], z2 = wz[iz + 1];
-                        float acc = rp[l];
-                        acc = fmaf(k01.x, wxp[m + SX - xps], acc);
-                        acc = fmaf(k01.y, wxm[m - SX - xms], acc);
-                        acc = fmaf(k23.x, wz[iz + H], acc);
-                        acc = fmaf(k23.y, wz[iz - H], acc);
-                        acc = fmaf(k45.x, odd ? z2 : z1, acc);
-                        acc = fmaf(k45.y, odd ? z1 : z0, acc);
-                        const float na = fmaf(sor, acc - old, old);
-                        dw[m] = na;
-                        const float ch = na - old;
-                        d2 = fmaf(ch, ch, d2);
-                        dd = fmaf(na, na, dd);
+            if (producer) {
+                if (lane == 0) {
+                    // the other colour was written (generic stores) before
+                    // the grid barrier; the copies read it through the async proxy
+                    fence_proxy_async();
+                    for (long long i = 0; i < mine; ++i, ++issued) {
+                        const unsigned s = issued % kTmaStages;
+                        if (issued >= (unsigned)kTmaStages &&
+                            !mbar_wait_flag(&empty[s], (issued / kTmaStages - 1) & 1u, err))
+                            break;
+                        const long long m0 = (b + i * nb) * C;
+                        const long long cnt = (N - m0) < C ? (N - m0) : C;   // % 32 == 0
+                        unsigned char* stg = smem + (size_t)s * T.bytes;
+                        tma_issue_own(c, T, stg, &full[s], Kc, dw, msk, m0, cnt);
+                        tma_issue_windows(c, T, stg, &full[s], dq, m0);
                     }
                 }
-                __syncthreads();   // stage s is free again
-                if (tid == 0 && i + kTmaStages < mine) {
-                    const long long qn = b + (i + kTmaStages) * nb;
-                    tma_issue_own(c, T, stg, &mbar[s], Kc, dw, msk, qn);
-                    tma_issue_windows(c, T, stg, &mbar[s], dq, qn);
+                __syncwarp();
+            } else {
+                for (long long i = group; i < mine; i += 2) {
+                    const unsigned u = uses + (unsigned)i;
+                    const unsigned s = u % kTmaStages;
+                    if (!mbar_wait_flag(&full[s], (u / kTmaStages) & 1u, err)) break;
+                    const unsigned char* stg = smem + (size_t)s * T.bytes;
+                    const long long m0 = (b + i * nb) * C;
+                    const int nval = (int)((Nc - m0) < C ? (Nc - m0) : C);
+                    // window offsets of cell l of the chunk (32-bit from here on)
+                    const int oz = (int)(m0 - ((m0 - H - 1) & ~3LL));
+                    const int oxp = (int)(m0 + SX - ((m0 + SX) & ~3LL));
+                    const int oxm = (int)(m0 - SX - ((m0 - SX) & ~3LL));
+                    const float2* rec = reinterpret_cast<const float2*>(stg + T.rec);
+                    const float* rp = reinterpret_cast<const float*>(stg + T.rp);
+                    const uint8_t* fl = stg + T.msk;
+                    const float* dwo = reinterpret_cast<const float*>(stg + T.dw);
+                    const float* wz = reinterpret_cast<const float*>(stg + T.wz);
+                    const float* wxp = reinterpret_cast<const float*>(stg + T.wxp);
+                    const float* wxm = reinterpret_cast<const float*>(stg + T.wxm);
+                    float* out = dw + m0;
+#pragma unroll
+                    for (int r = 0; r < kTmaCellsPerThread; ++r) {
+                        const int l = gt + r * kTmaGroup;
+                        if (l < nval) {
+                            const float2 k01 = rec[3 * l], k23 = rec[3 * l + 1], k45 = rec[3 * l + 2];
+                            const bool odd = (fl[l] & F_KODD) != 0;
+                            const float old = dwo[l];
+                            const int iz = l + oz;
+                            const float z0 = wz[iz - 1], z1 = wz[iz], z2 = wz[iz + 1];
+                            float acc = rp[l];
+                            acc = fmaf(k01.x, wxp[l + oxp], acc);
+                            acc = fmaf(k01.y, wxm[l + oxm], acc);
+                            acc = fmaf(k23.x, wz[iz + H], acc);
+                            acc = fmaf(k23.y, wz[iz - H], acc);
+                            acc = fmaf(k45.x, odd ? z2 : z1, acc);
+                            acc = fmaf(k45.y, odd ? z1 : z0, acc);
+                            const float na = fmaf(sor, acc - old, old);
+                            st_hint(out + l, na, keep);
+                            const float ch = na - old;
+                            d2 = fmaf(ch, ch, d2);
+                            dd = fmaf(na, na, dd);
+                        }
+                    }
+                    // the warp's reads of the stage are done: release it
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&empty[s]);
                 }
             }
-            if (!ok) break;
             uses += (unsigned)mine;
             // this phase's stores are read by the next phase's copies
             fence_proxy_async();
-            // own parts of the next phase's first chunks go out before the
-            // barrier (after the last iteration's second phase they are
-            // unused and drained at exit)
-            if (tid == 0) {
-                const int nc = 1 - col;
-                for (long long i = 0; i < pro; ++i) {
-                    const unsigned s = (uses + (unsigned)i) % kTmaStages;
-                    tma_issue_own(c, T, smem + (size_t)s * T.bytes, &mbar[s], c.K[nc], c.D[nc],
-                                  c.mask[nc], b + i * nb);
-                }
-            }
-            primed = true;
+            __syncthreads();
+            if (*err) { ok = false; break; }   // block-uniform after the barrier
             if (col == 1 && check) {
-                const double b1 = block_sum<kTmaBlock>((double)d2, sh);
-                const double b3 = block_sum<kTmaBlock>((double)dd, sh);
+                const double b1 = block_sum<kTmaThreads>((double)d2, sh);
+                const double b3 = block_sum<kTmaThreads>((double)dd, sh);
                 if (tid == 0) {
                     c.partials[4 * b + 2 * (checkno & 1)] = b1;
                     c.partials[4 * b + 2 * (checkno & 1) + 1] = b3;
@@ -551,8 +611,8 @@ __global__ void __launch_bounds__(kTmaBlock, TSE_TMA_MINB) dc_sweep_tma_kernel(D
                 s1 = s1 + __ldcg(c.partials + 4 * q + 2 * (checkno & 1));
                 s3 = s3 + __ldcg(c.partials + 4 * q + 2 * (checkno & 1) + 1);
             }
-            s1 = block_sum<kTmaBlock>(s1, sh);
-            s3 = block_sum<kTmaBlock>(s3, sh);
+            s1 = block_sum<kTmaThreads>(s1, sh);
+            s3 = block_sum<kTmaThreads>(s3, sh);
             if (tid == 0) {
                 sh[0] = s1;
                 sh[1] = s3;
@@ -586,19 +646,13 @@ __global__ void __launch_bounds__(kTmaBlock, TSE_TMA_MINB) dc_sweep_tma_kernel(D
         if (halved) { event = EV_HALVE; break; }
         if (refresh) { event = EV_REFRESH; break; }
     }
-    if (tid == 0) {
-        // let every copy this block issued land before its shared memory is
-        // released (bounded, like every wait here): primed stages get their
-        // missing arrival, so their phase completes once their bytes are in
-        if (event == EV_ERROR) atomicExch(&c.bar->error, 1);
-        for (unsigned u = drain_lo; u < drain_hi; ++u)
-            mbar_wait_bounded(&mbar[u % kTmaStages], (u / kTmaStages) & 1u);
-        if (primed)
-            for (long long i = 0; i < pro; ++i) {
-                const unsigned u = uses + (unsigned)i;
-                mbar_arrive(&mbar[u % kTmaStages]);
-                mbar_wait_bounded(&mbar[u % kTmaStages], (u / kTmaStages) & 1u);
-            }
+    if (event == EV_ERROR && producer && lane == 0) {
+        // the last copies issued into each stage must land before the
+        // block's shared memory is released (bounded waits, flag ignored)
+        atomicExch(&c.bar->error, 1);
+        const unsigned first = issued > (unsigned)kTmaStages ? issued - kTmaStages : 0u;
+        for (unsigned v = first; v < issued; ++v)
+            mbar_wait_bounded(&full[v % kTmaStages], (v / kTmaStages) & 1u);
     }
     if (leader) {
         st->t = t;
@@ -675,7 +729,7 @@ static int tma_blocks(long long Nc, int cap, size_t smem) {
     // below another's launch
     if (cudaFuncSetAttribute(dc_sweep_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)kTmaMaxSmem) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dc_sweep_tma_kernel, kTmaBlock, smem) !=
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dc_sweep_tma_kernel, kTmaThreads, smem) !=
             cudaSuccess ||
         per_sm < 1) {
         cudaGetLastError();
@@ -757,7 +811,7 @@ static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, 
         }
         const cudaError_t le =
             nb_tma > 0 ? cudaLaunchCooperativeKernel((const void*)dc_sweep_tma_kernel, dim3(nb),
-                                                     dim3(kTmaBlock), targs, tma_smem, stream)
+                                                     dim3(kTmaThreads), targs, tma_smem, stream)
                        : cudaLaunchCooperativeKernel((const void*)dc_sweep_kernel, dim3(nb),
                                                      dim3(kSweepBlock), args, 0, stream);
         if (le != cudaSuccess) {
