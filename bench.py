@@ -45,7 +45,7 @@ ALG_BYTES = {"fp64": 57, "fp32dc": 29}
 # dram__bytes_write.sum of one 64-iteration launch on the 192x192x128
 # reservoir, divided by its cell-updates; summaries under profiles/), scaled
 # to a launch of the benchmark by its cell-updates
-TRAFFIC_BYTES = {"fp32dc": 34.0, "fp64": 114.4}
+TRAFFIC_BYTES = {"fp32dc": 28.7, "fp64": 114.4}
 DEFAULT_SHAPE = (256, 256, 128)
 
 
@@ -415,14 +415,14 @@ def e2e_steps(ctx, sim, steps):
 
 def roofline(res, precision, peak, peak_kind):
     """Roofline of the dominant kernel: algorithmic bytes / event time.
-    fp32dc: the FP32 sweep kernel (dc_sweep_kernel, 96 % of device time);
+    fp32dc: the FP32 sweep kernel (dc_sweep_tma_kernel, 94 % of device time);
     fp64: the persistent FP64 solve (rb_solve_kernel, one launch per solve,
     timed with its assembly and unpack kernels)."""
     if precision == "fp32dc":
         if not res["n_s"]:
             return None
         units, ms, n = res["s_units"], res["s_ms"], res["n_s"]
-        name = "dc_sweep_kernel (FP32 correction sweeps)"
+        name = "dc_sweep_tma_kernel (FP32 correction sweeps, TMA-staged)"
     else:
         if not res["n_p"]:
             return None
