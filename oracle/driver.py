@@ -34,6 +34,45 @@ def pymin(*a):
     return m
 
 
+# the snapshot tuple of tse.py:324-326, in order
+SNAPSHOT_ITEMS = ("lx", "ly", "lz", "nx", "ny", "nz", "dx", "dy", "dz", "t_sim", "dt",
+                  "P", "C", "T", "qx", "qy", "qz", "phi", "Kx", "Ky", "Kz", "rho_f",
+                  "nue", "cp_f", "l_f", "BP", "BC", "BT", "L", "mass", "WP", "WT", "WC", "e")
+
+
+class Plots:
+    """plotresults (tse.py:312-329): with PLOTSAVE, shorten dt so the run
+    lands on the next PLOTTIME (remembering the unshortened dt in dt_prev);
+    on landing exactly, write the snapshot tuple with joblib (compress=3) to
+    "<prefix>-<index:05d>.p" and restore dt = dt_prev.  A time that is passed
+    without an exact landing is never written, and neither is any later one
+    (the index stays), as in the reference."""
+
+    def __init__(self, config, prefix):
+        self.on = bool(getattr(config, "PLOTSAVE", False))
+        self.times = getattr(config, "PLOTTIME", []) if self.on else []
+        self.index = 0
+        self.prefix = prefix
+        self.written = []
+
+    def __call__(self, t_sim, dt, dt_prev, items):
+        """items(dt) -> the 34-tuple; returns the new (dt, dt_prev)."""
+        if not self.on or self.index > numpy.shape(self.times)[0] - 1:
+            return dt, dt_prev
+        t_plot = self.times[self.index]
+        if t_sim < t_plot:
+            dt_prev = dt
+            dt = pymin(dt, t_plot - t_sim)
+        elif t_sim == t_plot:
+            import joblib
+            path = "{:s}-{:05d}.p".format(self.prefix, self.index)
+            joblib.dump(items(dt), path, compress=3)
+            self.written.append(path)
+            dt = dt_prev
+            self.index += 1
+        return dt, dt_prev
+
+
 def run_fluid_properties(config, S, T3):
     """Per-cell EOS callback over all cells (tse.py:179-199)."""
     C, P, nue, rho_f = S["C"], S["P"], S["nue"], S["rho_f"]
@@ -60,8 +99,10 @@ def update_fluid_properties(config, S):
     run_fluid_properties(config, S, T if T.ndim == 3 else T[:, :, :, 0])
 
 
-def run(config, max_steps=None, on_step=None, verbose=False):
-    """Run the config; returns the final state dict (plus 'n_tsteps', 't_sim')."""
+def run(config, max_steps=None, on_step=None, verbose=False, plot_prefix=None):
+    """Run the config; returns the final state dict (plus 'n_tsteps', 't_sim',
+    'plots' = snapshot files written).  Snapshots go to
+    "<plot_prefix>-<k:05d>.p" (default: the config module's name)."""
     if config.CHEMREACT:
         raise NotImplementedError("chemistry coupling is outside the time-step core")
     S = {}
@@ -101,6 +142,15 @@ def run(config, max_steps=None, on_step=None, verbose=False):
     Cn = S["C"].copy()
     Tn = S["T"].copy()
     log = []
+    plots = Plots(config, plot_prefix if plot_prefix is not None else config.__name__)
+
+    def snapshot(dt_now):
+        v = dict(lx=config.lx, ly=config.ly, lz=config.lz, nx=nx, ny=ny, nz=nz,
+                 dx=config.dx, dy=config.dy, dz=config.dz, t_sim=t_sim, dt=dt_now)
+        return tuple(v[k] if k in v else S[k] for k in SNAPSHOT_ITEMS)
+
+    dt_prev = dt                     # tse.py:1121
+    dt, dt_prev = plots(t_sim, dt, dt_prev, snapshot)   # tse.py:1177
     while t_sim < t:
         SIA_filled = False
         SIA_iter = 0
@@ -246,9 +296,11 @@ def run(config, max_steps=None, on_step=None, verbose=False):
             dt = pymin(dt_T, t - t_sim, dt)
         if config.SPECTRANS:
             dt = pymin(dt_C, t - t_sim, dt)
+        dt, dt_prev = plots(t_sim, dt, dt_prev, snapshot)   # tse.py:1494
         if max_steps is not None and n_tsteps >= max_steps:
             break
     S["t_sim"] = t_sim
     S["n_tsteps"] = n_tsteps
+    S["plots"] = list(plots.written)
     S["log"] = log
     return S

@@ -79,8 +79,16 @@ def reference_namespace(ref, cfg):
     return _exec_reference(ref, cfg)
 
 
+# the snapshot tuple of tse.py:324-326, in order
+SNAPSHOT_ITEMS = ("lx", "ly", "lz", "nx", "ny", "nz", "dx", "dy", "dz", "t_sim", "dt",
+                  "P", "C", "T", "qx", "qy", "qz", "phi", "Kx", "Ky", "Kz", "rho_f",
+                  "nue", "cp_f", "l_f", "BP", "BC", "BT", "L", "mass", "WP", "WT", "WC", "e")
+
+
 def run_reference(ref, cfg, steps, keep_steps, fields):
-    """Run ``steps`` time steps; record scalars every step, fields at keep_steps."""
+    """Run ``steps`` time steps; record scalars every step, fields at keep_steps.
+    With PLOTSAVE on, the run happens in a scratch directory and the snapshot
+    files tse.py writes there are recorded item by item ("plot<k>_<item>")."""
     rec = {"dt": [], "t_sim": [], "numitP": [], "numitC": [], "numitT": [],
            "num_CFL": [], "dt_P": [], "dt_C": [], "dt_T": []}
     snaps = {}
@@ -100,8 +108,32 @@ def run_reference(ref, cfg, steps, keep_steps, fields):
         return bc_inc, P, T, C, BP, BT, BC, WP, WT, WC, Kx, Ky, Kz
 
     cfg.dynamic_bc = dynamic_bc
-    ns = _exec_reference(ref, cfg)
+    plots = {}
+    if getattr(cfg, "PLOTSAVE", False):
+        import glob
+        import joblib
+        import tempfile
+        cwd = os.getcwd()
+        with tempfile.TemporaryDirectory() as tmp:
+            os.chdir(tmp)
+            try:
+                ns = _exec_reference(ref, cfg)
+                files = sorted(glob.glob("*-[0-9][0-9][0-9][0-9][0-9].p"))
+                for k, f in enumerate(files):
+                    for name, v in zip(SNAPSHOT_ITEMS, joblib.load(f)):
+                        # later files keep only the items that differ from the
+                        # first file's (a missing key means "as in plot0")
+                        v = numpy.array(v)
+                        p0 = plots.get("plot0_" + name)
+                        if k == 0 or not (p0.shape == v.shape and numpy.array_equal(p0, v)):
+                            plots["plot%d_%s" % (k, name)] = v
+            finally:
+                os.chdir(cwd)
+        plots["n_plots"] = numpy.array(len(files))
+    else:
+        ns = _exec_reference(ref, cfg)
     out = {("s_" + k): numpy.array(v) for k, v in rec.items()}
+    out.update(plots)
     out.update(snaps)
     out["keep_steps"] = numpy.array(sorted(keep_steps))
     out["steps"] = numpy.array(steps)
@@ -138,6 +170,7 @@ E2E = {
                         6, {1, 3, 6}, ("P", "C", "T", "qx", "qy", "qz")),
     "serving_request": (workloads.serving_request, {"seed": 4, "n": 9},
                         5, {1, 5}, ("P", "C", "T", "qz")),
+    "slice_2d_plot": (workloads.slice_2d_plot, {}, 100, {1, 50, 100}, ("P", "C", "qx", "qz")),
 }
 
 

@@ -75,3 +75,27 @@ def model_for(cfg, device, precision="fp64"):
     m.freeze(cfg.c_r, cfg.l_r, cfg.rho_r, cfg.cp_r, cfg.lf_l, cfg.lf_t, cfg.lt_l, cfg.lt_t,
              cfg.C_IMBLFLO, cfg.T_IMBLFLO)
     return m
+
+
+def check_snapshots(files, fx, tol):
+    """The snapshot files a run wrote against the reference's (fixture keys
+    "plot<k>_<item>", a missing key meaning "as in plot0"): same count, same
+    tuple layout, integers and flags equal, floating-point items within
+    ``tol`` relative to each item's scale (0: bit for bit)."""
+    import joblib
+    from tests.golden.make_golden import SNAPSHOT_ITEMS
+    n = int(fx["n_plots"])
+    assert len(files) == n, (len(files), n)
+    for k, f in enumerate(files):
+        assert f.endswith("-%05d.p" % k), f
+        got = joblib.load(f)
+        assert len(got) == len(SNAPSHOT_ITEMS)
+        for name, v in zip(SNAPSHOT_ITEMS, got):
+            key = "plot%d_%s" % (k, name)
+            ref = fx[key] if key in fx.files else fx["plot0_" + name]
+            v = numpy.asarray(v)
+            assert v.shape == ref.shape, (k, name, v.shape, ref.shape)
+            if tol == 0 or name in ("nx", "ny", "nz", "BP", "BC", "BT", "t_sim"):
+                assert numpy.array_equal(v, ref), (k, name)
+            else:
+                assert rel_err(v, ref) <= tol, (k, name, rel_err(v, ref))

@@ -12,7 +12,7 @@ import pytest
 from oracle.oracle import OracleModel
 from tests.golden import cases
 from tests.golden.make_golden import E2E
-from tests.helpers import NumpyKernels, load, model_for, rel_err
+from tests.helpers import NumpyKernels, check_snapshots, load, model_for, rel_err
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-6
@@ -72,7 +72,7 @@ def test_dc_pressure_vs_oracle(shape, cuda_device):
 
 
 @pytest.mark.parametrize("name", sorted(E2E))
-def test_dc_driver_matches_reference_run(name, cuda_device):
+def test_dc_driver_matches_reference_run(name, cuda_device, tmp_path):
     from transportse_b200.driver import Simulation
     builder, kw, steps, keep, fields = E2E[name]
     fx = load("e2e_" + name)
@@ -84,7 +84,11 @@ def test_dc_driver_matches_reference_run(name, cuda_device):
             for f in fields:
                 got["%s@%d" % (f, rec["step"])] = sim.field(f)
 
-    Simulation(cfg, device=cuda_device, precision="fp32dc").run(max_steps=steps, on_step=tap)
+    sim = Simulation(cfg, device=cuda_device, precision="fp32dc",
+                     plot_prefix=str(tmp_path / "snap"))
+    sim.run(max_steps=steps, on_step=tap)
+    if "n_plots" in fx.files:
+        check_snapshots(sim.plots.written, fx, TOL)
     for k in fx.files:
         if "@" in k and k.split("@")[0] in ("P", "C", "T"):
             e = rel_err(got[k], fx[k])

@@ -7,14 +7,14 @@ import pytest
 
 from tests.golden import cases
 from tests.golden.make_golden import E2E
-from tests.helpers import load, rel_err
+from tests.helpers import check_snapshots, load, rel_err
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-9
 
 
 @pytest.mark.parametrize("name", sorted(E2E))
-def test_driver_matches_reference_run(name, cuda_device):
+def test_driver_matches_reference_run(name, cuda_device, tmp_path):
     from transportse_b200.driver import Simulation
     builder, kw, steps, keep, fields = E2E[name]
     fx = load("e2e_" + name)
@@ -30,7 +30,10 @@ def test_driver_matches_reference_run(name, cuda_device):
             for f in fields:
                 got["%s@%d" % (f, rec["step"])] = sim.field(f)
 
-    Simulation(cfg, device=cuda_device).run(max_steps=steps, on_step=tap)
+    sim = Simulation(cfg, device=cuda_device, plot_prefix=str(tmp_path / "snap"))
+    sim.run(max_steps=steps, on_step=tap)
+    if "n_plots" in fx.files:
+        check_snapshots(sim.plots.written, fx, TOL)
     for k in ("numitP", "numitC", "numitT", "num_CFL"):
         assert numpy.array_equal(numpy.array(scal[k]), fx["s_" + k]), k
     for k in ("dt", "t_sim"):

@@ -150,3 +150,33 @@ def test_batch_gate_launches_when_every_member_waits(monkeypatch):
     # the rest flush once the third member has left
     assert sum(len(x) for x in launched) == 5
     assert gate.members == 0 and gate.running == 0
+
+
+def test_snapshot_rule_matches_the_oracle(tmp_path):
+    """driver.Snapshots (product) and oracle.driver.Plots (restatement of
+    tse.py:312-329) give the same dt sequence and files, including a plot time
+    that a step passes without landing on it (that one and all later ones are
+    never written)."""
+    import types
+    import numpy
+    from oracle.driver import Plots
+    from transportse_b200.driver import Snapshots
+
+    for times in ([0.0, 10.0, 25.0, 40.0], [5.0, 7.3, 100.0], [3.0, 3.5]):
+        cfg = types.SimpleNamespace(PLOTSAVE=True, PLOTTIME=numpy.array(times))
+        outs = []
+        for k, cls in enumerate((Snapshots, Plots)):
+            pl = cls(cfg, str(tmp_path / ("r%d" % k)))
+            step = pl.step if cls is Snapshots else pl.__call__
+            t_sim, dt = 0.0, 4.0
+            dt, dt_prev = step(t_sim, dt, dt, lambda d: (t_sim, d))
+            seq = []
+            for n in range(30):
+                seq.append(dt)
+                t_sim += dt
+                dt = 4.0 if n % 3 else 6.5          # the solvers' next dt
+                if n == 4 and times[0] == 3.0:
+                    t_sim += 0.25                    # step over a plot time
+                dt, dt_prev = step(t_sim, dt, dt_prev, lambda d, t=t_sim: (t, d))
+            outs.append((seq, [p[-8:] for p in pl.written], pl.index))
+        assert outs[0] == outs[1], times

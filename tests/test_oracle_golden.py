@@ -8,7 +8,7 @@ from oracle import driver as odriver
 from oracle.oracle import OracleModel
 from tests.golden import cases
 from tests.golden.make_golden import E2E
-from tests.helpers import load
+from tests.helpers import check_snapshots, load
 
 
 @pytest.mark.parametrize("variant", ["a", "b"])
@@ -26,7 +26,7 @@ def test_oracle_unit_kernels_bit_exact(variant):
 
 
 @pytest.mark.parametrize("name", sorted(E2E))
-def test_oracle_driver_bit_exact(name):
+def test_oracle_driver_bit_exact(name, tmp_path):
     builder, kw, steps, keep, fields = E2E[name]
     fx = load("e2e_" + name)
     cfg = builder(**kw)
@@ -41,7 +41,9 @@ def test_oracle_driver_bit_exact(name):
             for f in fields:
                 got["%s@%d" % (f, rec["step"])] = S[f].copy()
 
-    odriver.run(cfg, max_steps=steps, on_step=tap)
+    S = odriver.run(cfg, max_steps=steps, on_step=tap, plot_prefix=str(tmp_path / "snap"))
+    if "n_plots" in fx.files:
+        check_snapshots(S["plots"], fx, 0)
     for k, v in scal.items():
         assert numpy.array_equal(numpy.array(v), fx["s_" + k]), k
     for k in fx.files:

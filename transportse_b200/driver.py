@@ -36,6 +36,46 @@ FIELDS3 = ("phi", "Kx", "Ky", "Kz", "c_r", "cp_r", "l_r", "rho_r", "lf_l", "lf_t
            "WT", "qx", "qy", "qz")
 FIELDS4 = ("D_fx", "D_fy", "D_fz", "C", "WC")
 
+# the snapshot tuple tse2pvd.py reads (tse.py:324-326), in order
+SNAPSHOT_ITEMS = ("lx", "ly", "lz", "nx", "ny", "nz", "dx", "dy", "dz", "t_sim", "dt",
+                  "P", "C", "T", "qx", "qy", "qz", "phi", "Kx", "Ky", "Kz", "rho_f",
+                  "nue", "cp_f", "l_f", "BP", "BC", "BT", "L", "mass", "WP", "WT", "WC", "e")
+
+
+class Snapshots:
+    """Result snapshots at the PLOTTIME list (plotresults, tse.py:312-329).
+
+    With PLOTSAVE on, the step before a plot time is shortened so the run
+    lands on it (the unshortened dt is remembered); at a landing the fields
+    come to the host once and the tuple is written with joblib (compress=3)
+    to "<prefix>-<index:05d>.p", and dt returns to the remembered value.  A
+    plot time that is stepped over without an exact landing is not written,
+    and then no later one is either -- the reference behaves the same way."""
+
+    def __init__(self, config, prefix):
+        self.on = bool(getattr(config, "PLOTSAVE", False))
+        self.times = getattr(config, "PLOTTIME", []) if self.on else []
+        self.index = 0
+        self.prefix = prefix
+        self.written = []
+
+    def step(self, t_sim, dt, dt_prev, items):
+        """items(dt) builds the tuple; returns the new (dt, dt_prev)."""
+        if not self.on or self.index > numpy.shape(self.times)[0] - 1:
+            return dt, dt_prev
+        t_plot = self.times[self.index]
+        if t_sim < t_plot:
+            dt_prev = dt
+            dt = pymin(dt, t_plot - t_sim)
+        elif t_sim == t_plot:
+            import joblib
+            path = "{:s}-{:05d}.p".format(self.prefix, self.index)
+            joblib.dump(items(dt), path, compress=3)
+            self.written.append(path)
+            dt = dt_prev
+            self.index += 1
+        return dt, dt_prev
+
 
 class ConvergenceError(SystemExit):
     pass
@@ -50,10 +90,11 @@ def pymin(*a):
 
 
 class Simulation:
-    def __init__(self, config, device=None, verbose=False, precision=None):
+    def __init__(self, config, device=None, verbose=False, precision=None, plot_prefix=None):
         """precision: 'fp64' (the reference's arithmetic) or 'fp32dc' (FP32
         sweeps with FP64 defect correction); default: config.GPU_PRECISION,
-        else 'fp64'."""
+        else 'fp64'.  plot_prefix: path prefix of the PLOTSAVE snapshot files
+        (default: the config module's name, in the working directory)."""
         if config.CHEMREACT:
             raise NotImplementedError("CHEMREACT: chemistry coupling is not part of the GPU "
                                       "time-step core")
@@ -89,6 +130,8 @@ class Simulation:
         self.log = []
         self.mass_log = []
         self.counters = dict(P=0, C=0, T=0)
+        self.plots = Snapshots(config, plot_prefix if plot_prefix is not None
+                               else getattr(config, "__name__", "tse"))
 
     # ------------------------------------------------------------ state I/O
     def upload_state(self, config):
@@ -122,10 +165,21 @@ class Simulation:
             _eos.host_callback(self, T0)
 
     # ----------------------------------------------------------------- loop
+    def snapshot(self, dt):
+        """The snapshot tuple of the current state (host copies)."""
+        cfg = self.config
+        v = dict(lx=cfg.lx, ly=cfg.ly, lz=cfg.lz, nx=self.shape[0], ny=self.shape[1],
+                 nz=self.shape[2], dx=cfg.dx, dy=cfg.dy, dz=cfg.dz, t_sim=self.t_sim, dt=dt,
+                 mass=getattr(self, "mass", cfg.mass))
+        return tuple(v[k] if k in v else self.field(k) for k in SNAPSHOT_ITEMS)
+
     def _init_loop(self):
         cfg, S = self.config, self.S
         self._L = dict(dt_max=cfg.dt_max, dt=cfg.dt, dt_P=None, dt_C=None, dt_T=None, num_CFL=0,
                        pe=(0.0,) * 6)
+        # tse.py:1121 and the call before the loop, tse.py:1177
+        self._L["dt"], self._L["dt_prev"] = self.plots.step(self.t_sim, cfg.dt, cfg.dt,
+                                                            self.snapshot)
         self._rhof_prev = torch.zeros_like(S["rho_f"])
         self._Cn = torch.empty_like(S["C"])
         self._Tn = torch.empty_like(S["T"])
@@ -140,7 +194,7 @@ class Simulation:
         dt_max = Ls["dt_max"]
         cmax_dt = cfg.dt_max
         dt_max_abs = cfg.dt_max
-        dt = Ls["dt"]
+        dt, dt_prev = Ls["dt"], Ls["dt_prev"]
         dt_P, dt_C, dt_T = Ls["dt_P"], Ls["dt_C"], Ls["dt_T"]
         num_CFL = Ls["num_CFL"]
         rhof_prev = self._rhof_prev
@@ -325,10 +379,11 @@ class Simulation:
                     raise RuntimeError("name 'dt_C' is not defined: no species was transported "
                                        "in the first step (the reference stops here as well)")
                 dt = pymin(dt_C, t - self.t_sim, dt)
+            dt, dt_prev = self.plots.step(self.t_sim, dt, dt_prev, self.snapshot)   # tse.py:1494
             if max_steps is not None and steps_here >= max_steps:
                 break
-        Ls.update(dt_max=dt_max, dt=dt, dt_P=dt_P, dt_C=dt_C, dt_T=dt_T, num_CFL=num_CFL,
-                  pe=(Pex_T, Pey_T, Pez_T, Pex_C, Pey_C, Pez_C))
+        Ls.update(dt_max=dt_max, dt=dt, dt_prev=dt_prev, dt_P=dt_P, dt_C=dt_C, dt_T=dt_T,
+                  num_CFL=num_CFL, pe=(Pex_T, Pey_T, Pez_T, Pex_C, Pey_C, Pez_C))
         return self
 
     # -------------------------------------------------------------- hooks
@@ -411,7 +466,8 @@ def main(argv=None):
     spec = importlib.util.spec_from_file_location(os.path.basename(path)[:-3], path)
     cfg = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(cfg)
-    sim = Simulation(cfg, verbose=not a.quiet)
+    # snapshots next to the config file, named like the reference's
+    sim = Simulation(cfg, verbose=not a.quiet, plot_prefix=path[:-3])
     sim.run(max_steps=a.steps)
     print("[ SIMULATION SUMMARY ]")
     print("[t/s] %8.2e/%8.2e [S] %5d [P] %5d [C] %5d [T] %5d"

@@ -49,9 +49,9 @@ class Model:
         self.nx, self.ny, self.nz = int(nx), int(ny), int(nz)
         self.n = self.nx * self.ny * self.nz
         f64 = dict(dtype=torch.float64, device=self.device)
-        self.dx = torch.as_tensor(numpy.ascontiguousarray(dx, dtype=numpy.float64), **f64)
-        self.dy = torch.as_tensor(numpy.ascontiguousarray(dy, dtype=numpy.float64), **f64)
-        self.dz = torch.as_tensor(numpy.ascontiguousarray(dz, dtype=numpy.float64), **f64)
+        self.dx = torch.as_tensor(numpy.array(dx, dtype=numpy.float64), **f64)
+        self.dy = torch.as_tensor(numpy.array(dy, dtype=numpy.float64), **f64)
+        self.dz = torch.as_tensor(numpy.array(dz, dtype=numpy.float64), **f64)
         self.g = float(g)
         self.sinb, self.cosb = _sin_cos_beta(beta_deg)
         self.grid = N.TseGrid(self.nx, self.ny, self.nz, 0, self.dx.data_ptr(),

@@ -209,6 +209,17 @@ def slice_2d(nx=60, ny=1, nz=30, steps=200):
     return m
 
 
+def slice_2d_plot(nx=60, ny=1, nz=30, steps=100, t_last=2.0e7, n_plot=6):
+    """slice_2d with snapshots on, as the course configs run: PLOTSAVE = True
+    and PLOTTIME = linspace(0, 1, n_plot) * t_last, so the step sequence is
+    shortened to land on every plot time (tse.py:312-329)."""
+    m = slice_2d(nx, ny, nz, steps)
+    m.__name__ = "slice_2d_plot"
+    m.PLOTSAVE = True
+    m.PLOTTIME = numpy.linspace(0.0, 1.0, n_plot) * t_last
+    return m
+
+
 def reservoir_3d(nx=256, ny=256, nz=128, seed=2024, steps=100):
     """Bottom-heated 3-D reservoir with a dense brine patch on top.
 
