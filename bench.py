@@ -116,12 +116,17 @@ def bench_ensemble(a):
     _, st = Ensemble(cfgs, device=dev, precision="fp32dc", dc_cycle=cyc, **kw).run(a.steps, keep=())
     clk = clocks.stop()
     cells = [c.nx * c.ny * c.nz for c in cfgs]
+    value = st["stepping_cell_updates_per_s"] or st["cell_updates_per_s"]
     print(json.dumps({
-        "metric": "SOR cell-updates/s", "value": st["cell_updates_per_s"], "unit": "cell-updates/s",
+        "metric": "SOR cell-updates/s", "value": value, "unit": "cell-updates/s",
         "n_gpus": 1, "steps": a.steps, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "ensemble of %d models, axes log-uniform 32-%d, %d steps each, "
-                               "FP32 sweeps + FP64 defect correction" % (a.models, nmax, a.steps),
+                               "FP32 sweeps + FP64 defect correction; value = cell-updates over "
+                               "the stepping phase (one-time model set-up in setup_s)"
+                               % (a.models, nmax, a.steps),
                    "cells_total": int(sum(cells)), "cells_max": int(max(cells))},
+        "setup_s": st["setup_s"], "step_s": st["step_s"],
+        "with_setup_cell_updates_per_s": st["cell_updates_per_s"],
         "wall_s": st["wall_s"], "batched": batched, "cluster": cl, "concurrency": st["concurrency"],
         "dc_cycle": cyc, "max_blocks": st["max_blocks"], "batch": st["batch"],
         "autotune": tune, "clocks": clk}))

@@ -163,16 +163,21 @@ int32_t tse_compute_T_dc(const TseGrid *grid, const TseHeatArgs *args,
 
 /* Batched mixed-precision solves: the compute_P / compute_C / compute_T
  * calls of n independent models (an ensemble, or the requests a server is
- * stepping together), run as one persistent launch with one thread-block
- * cluster per model.  Each item is exactly the single-model call of
+ * stepping together).  Each item is exactly the single-model call of
  * tse_compute_*_dc -- its own grid, arguments, status record and workspace
  * (TSE_WS_PRESSURE_DC / TSE_WS_TRANSPORT_DC; no two items may share one) --
  * and gets the same results to the solver tolerance.  opts->cycle as for the
- * single-model form; opts->max_blocks is the cluster size (CTAs per model,
- * <= 0: 8, at most 16); the timing fields are not written.  d_batch_ws holds
- * tse_batch_workspace_bytes(n) bytes.  The call returns after queueing the
- * work on `stream`; nothing is read back.  A non-finite dt or min_dt is
- * TSE_ERR_ARG.  Replaces n calls of tse.py:647 / 783 / 919. */
+ * single-model form; the timing fields are not written.
+ *   opts->max_blocks <= 0: fused form -- every model's cells in one
+ *     cooperative sweep sharing its barriers (models that finish drop out);
+ *     the call synchronises the stream once per launch and returns when
+ *     every solve is done;
+ *   opts->max_blocks > 0: cluster form -- one persistent launch with one
+ *     thread-block cluster of max_blocks CTAs (at most 16) per model; the
+ *     call returns after queueing the work, nothing is read back.
+ * d_batch_ws holds tse_batch_workspace_bytes(n, total_cells) bytes, where
+ * total_cells is the sum of nx*ny*nz over the items.  A non-finite dt or
+ * min_dt is TSE_ERR_ARG.  Replaces n calls of tse.py:647 / 783 / 919. */
 typedef struct TseBatchPressure {
     const TseGrid *grid;
     const TsePressureArgs *args;
@@ -194,7 +199,7 @@ typedef struct TseBatchHeat {
     void *d_workspace;
     size_t workspace_bytes;
 } TseBatchHeat;
-size_t tse_batch_workspace_bytes(int32_t n);
+size_t tse_batch_workspace_bytes(int32_t n, int64_t total_cells);
 int32_t tse_compute_P_dc_batch(const TseBatchPressure *items, int32_t n,
                                const TseDcOptions *opts, void *d_batch_ws,
                                size_t batch_ws_bytes, void *stream);

@@ -81,7 +81,7 @@ def test_ops_fail_loudly_without_library(monkeypatch):
 def test_batch_entry_points_validate_without_gpu():
     """Argument errors return TSE_ERR_ARG before any device call."""
     L = N.lib()
-    assert L.tse_batch_workspace_bytes(4) >= 256
+    assert L.tse_batch_workspace_bytes(4, 4096) >= 256
     opts = N.TseDcOptions(128, 8, 0)
     g = N.TseGrid(8, 8, 8, 0, None, None, None, 9.81, 0.0, 1.0)
     ws = ct.c_void_p(4096)   # never dereferenced: validation fails first

@@ -102,7 +102,7 @@ SIGNATURES = {
                               _S, _P]),
     "tse_compute_T_dc": (_I, [_G, ct.POINTER(TseHeatArgs), ct.POINTER(TseDcOptions), _P, _P, _S,
                               _P]),
-    "tse_batch_workspace_bytes": (ct.c_size_t, [_I]),
+    "tse_batch_workspace_bytes": (ct.c_size_t, [_I, ct.c_int64]),
     "tse_compute_P_dc_batch": (_I, [ct.POINTER(TseBatchPressure), _I, ct.POINTER(TseDcOptions), _P,
                                     _S, _P]),
     "tse_compute_C_dc_batch": (_I, [ct.POINTER(TseBatchSpecies), _I, ct.POINTER(TseDcOptions), _P,

@@ -127,8 +127,9 @@ class BatchGate:
             s = self.streams[key] = torch.cuda.Stream(device=self.device)
         return s
 
-    def _workspace(self, key, n, stream):
-        need = int(N.lib().tse_batch_workspace_bytes(n))
+    def _workspace(self, key, rs, stream):
+        cells = sum(r.grid.nx * r.grid.ny * r.grid.nz for r in rs)
+        need = int(N.lib().tse_batch_workspace_bytes(len(rs), cells))
         t = self.ws.get(key)
         if t is None or t.numel() < need:
             with torch.cuda.stream(stream):
@@ -148,7 +149,7 @@ class BatchGate:
                     if r.stream.cuda_stream not in seen:
                         seen.add(r.stream.cuda_stream)
                         bs.wait_stream(r.stream)
-                ws = self._workspace((name, cycle), len(rs), bs)
+                ws = self._workspace((name, cycle), rs, bs)
                 Item = N.BATCH_ITEM[name]
                 items = (Item * len(rs))(*[Item(ct.pointer(r.grid), ct.pointer(r.args),
                                                 ct.c_void_p(r.status.data_ptr()),

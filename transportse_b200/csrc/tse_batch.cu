@@ -328,13 +328,458 @@ static void fill_ctl(DcCtl& c, double inc_it, double max_dt, double min_dt, doub
 // NaN in dt or min_dt would keep a non-converging solve halving forever
 static bool finite_dt(double dt, double min_dt) { return std::isfinite(dt) && std::isfinite(min_dt); }
 
+// ====================================================== fused batched sweeps
+// All models of a batch in one cooperative sweep: the chunks (kTmaChunk
+// cells) of every active model form one table, interleaved over the blocks,
+// and every block runs the staged producer/consumer pipeline of
+// dc_sweep_tma_kernel over it, each chunk copied from its own model's arrays.
+// The models share the colour-phase barriers, so a small model costs its
+// bytes, not two device-wide barriers per iteration; a model that finishes
+// drops out of the table at the next launch and the rest keep the GPU.
+//
+// All active models advance one iteration per global iteration, so they
+// share the iteration count and the check schedule (pressure: every
+// iteration below 50, then every 10th; transport: every iteration).  At a
+// check each chunk stores its two colours' sums; after the barrier one block
+// per model adds its chunks in order and takes that model's decision
+// (converged, dt halving, stop, refresh, cycle end: the order of
+// dc_sweep_kernel); any event ends the launch after one more barrier.  A
+// model's cycle end and dt halving fall on iterations known in advance, so
+// the host bounds each launch by the nearest one and the decisions run there
+// too.  Between launches the host finishes each model's event with the
+// per-model steps of tse_dc.cu (x += d, residual, halving).
+struct FusedItem {
+    DcCtl c;
+    long long cfirst, nchunks;   // this model's chunks in the table
+    int inner;                   // iterations since its last residual, at launch
+    int pad;
+};
+
+struct FusedChunk {
+    long long m0;
+    int item;
+    int pad;
+};
+
+struct FusedArgs {
+    const FusedItem* items;
+    int nitems;
+    const FusedChunk* chunks;
+    long long nchunks;
+    double2* cpart;      // per chunk, colour and consumer warp: (sum of change^2, sum of d^2)
+    int* any_event;
+    GridBarrier* bar;
+    int g_max;           // iterations this launch runs at most
+    int num_it0;         // the models' iteration count at launch
+    int pressure_schedule;
+};
+
+// one model's decision after global iteration g (thread 0 of its block)
+__device__ void fused_decide(const FusedItem& I, int g, int num_it, bool check, double s1, double s3,
+                             int* any_event) {
+    const DcCtl& c = I.c;
+    DcState* st = c.st;
+    double t = st->t, dt = st->dt;
+    int sub = st->num_sub_it + (num_it - st->num_it);
+    const int inner = I.inner + g;
+    double diff = 1e100;
+    bool refresh = false;
+    if (check) {
+        const double l2 = sqrt(s1) / sqrt(st->x2 + 1e-200);
+        diff = (l2 != l2) ? 1.0 : l2;
+        refresh = sqrt(s1) < kRefresh * sqrt(s3);
+    }
+    int ev = EV_NONE;
+    if (diff < c.conv || c.stop_on_first) {
+        t += dt;
+        if (sub < c.max_it / 2.0) dt = pymin(dt * c.inc_it, c.max_dt);
+        ev = EV_CONVERGED;
+        st->converged = 1;
+    } else {
+        bool halved = false;
+        if (sub >= c.max_it) {
+            if (st->nev < 8) {
+                st->ev_it[st->nev] = num_it;
+                st->ev_dt[st->nev] = dt;
+                st->ev_diff[st->nev] = diff;
+            }
+            st->nev += 1;
+            dt = dt / 2;
+            sub = 0;
+            st->halvings += 1;
+            halved = true;
+        }
+        if (dt <= c.min_dt) ev = halved ? EV_STOP_HALVED : EV_STOP;
+        else if (halved) ev = EV_HALVE;
+        else if (refresh) ev = EV_REFRESH;
+        else if (inner >= c.cycle) ev = EV_CYCLE_END;
+    }
+    st->t = t;
+    st->dt = dt;
+    st->diff = diff;
+    st->num_it = num_it;
+    st->num_sub_it = sub;
+    st->event = ev;
+    if (ev != EV_NONE) atomicExch(any_event, 1);
+}
+
+__global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) fused_sweep_kernel(FusedArgs A, TmaStage T) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ __align__(8) uint64_t full[kTmaStages];
+    __shared__ __align__(8) uint64_t empty[kTmaStages];
+    __shared__ double sh[kTmaThreads / 32];
+    __shared__ int s_err;
+    const unsigned nb = gridDim.x, b = blockIdx.x;
+    const int tid = threadIdx.x;
+    const int warp = tid >> 5, lane = tid & 31;
+    const bool producer = warp == kTmaConsumers / 32;
+    const int group = warp >> 2;
+    const int gt = tid & (kTmaGroup - 1);
+    const long long C = kTmaChunk;
+    const long long mine = A.nchunks > (long long)b ? (A.nchunks - 1 - b) / nb + 1 : 0;
+    const uint64_t keep = l2_evict_last();
+    volatile int* err = &s_err;
+    if (tid == 0) {
+        for (int s = 0; s < kTmaStages; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], kTmaConsumers / 64);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        s_err = 0;
+    }
+    __syncthreads();
+    unsigned uses = 0, issued = 0;
+    bool ok = true;
+    for (int g = 1; g <= A.g_max && ok; ++g) {
+        const int num_it = A.num_it0 + g;
+        const bool check = A.pressure_schedule ? (num_it < 50 || num_it % 10 == 0) : true;
+        const bool last = g == A.g_max;
+        for (int col = 0; col < 2 && ok; ++col) {
+            if (producer) {
+                if (lane == 0) {
+                    fence_proxy_async();
+                    for (long long i = 0; i < mine; ++i, ++issued) {
+                        const unsigned s = issued % kTmaStages;
+                        if (issued >= (unsigned)kTmaStages &&
+                            !mbar_wait_flag(&empty[s], (issued / kTmaStages - 1) & 1u, err))
+                            break;
+                        const FusedChunk ch = A.chunks[b + i * nb];
+                        const DcCtl& c = A.items[ch.item].c;
+                        const long long cnt = (c.Ncal - ch.m0) < C ? (c.Ncal - ch.m0) : C;
+                        unsigned char* stg = smem + (size_t)s * T.bytes;
+                        tma_issue_own(c, T, stg, &full[s], c.K[col], c.D[col], c.mask[col], ch.m0, cnt);
+                        tma_issue_windows(c, T, stg, &full[s], c.D[1 - col], ch.m0);
+                    }
+                }
+                __syncwarp();
+            } else {
+                for (long long i = group; i < mine; i += 2) {
+                    const unsigned u = uses + (unsigned)i;
+                    const unsigned s = u % kTmaStages;
+                    // warp-uniform: lane 0 waits, the warp follows its outcome,
+                    // then every lane observes the completed phase (acquire)
+                    int okw = 1;
+                    if (lane == 0) okw = mbar_wait_flag(&full[s], (u / kTmaStages) & 1u, err);
+                    if (!__shfl_sync(0xffffffffu, okw, 0)) break;
+                    mbar_try_wait(&full[s], (u / kTmaStages) & 1u);
+                    const unsigned char* stg = smem + (size_t)s * T.bytes;
+                    const long long q = b + i * nb;
+                    const FusedChunk ch = A.chunks[q];
+                    const DcCtl& c = A.items[ch.item].c;
+                    const long long m0 = ch.m0, SX = c.L.SX;
+                    const int H = c.L.H;
+                    const float sor = c.sor;
+                    const int nval = (int)((c.L.Nc - m0) < C ? (c.L.Nc - m0) : C);
+                    const int oz = (int)(m0 - ((m0 - H - 1) & ~3LL));
+                    const int oxp = (int)(m0 + SX - ((m0 + SX) & ~3LL));
+                    const int oxm = (int)(m0 - SX - ((m0 - SX) & ~3LL));
+                    const float2* rec = reinterpret_cast<const float2*>(stg + T.rec);
+                    const float* rp = reinterpret_cast<const float*>(stg + T.rp);
+                    const uint8_t* fl = stg + T.msk;
+                    const float* dwo = reinterpret_cast<const float*>(stg + T.dw);
+                    const float* wz = reinterpret_cast<const float*>(stg + T.wz);
+                    const float* wxp = reinterpret_cast<const float*>(stg + T.wxp);
+                    const float* wxm = reinterpret_cast<const float*>(stg + T.wxm);
+                    float* out = c.D[col] + m0;
+                    float d2 = 0.0f, dd = 0.0f;
+#pragma unroll
+                    for (int r = 0; r < kTmaCellsPerThread; ++r) {
+                        const int l = gt + r * kTmaGroup;
+                        if (l < nval) {
+                            const float2 k01 = rec[3 * l], k23 = rec[3 * l + 1], k45 = rec[3 * l + 2];
+                            const bool odd = (fl[l] & F_KODD) != 0;
+                            const float old = dwo[l];
+                            const int iz = l + oz;
+                            const float z0 = wz[iz - 1], z1 = wz[iz], z2 = wz[iz + 1];
+                            float acc = rp[l];
+                            acc = fmaf(k01.x, wxp[l + oxp], acc);
+                            acc = fmaf(k01.y, wxm[l + oxm], acc);
+                            acc = fmaf(k23.x, wz[iz + H], acc);
+                            acc = fmaf(k23.y, wz[iz - H], acc);
+                            acc = fmaf(k45.x, odd ? z2 : z1, acc);
+                            acc = fmaf(k45.y, odd ? z1 : z0, acc);
+                            const float na = fmaf(sor, acc - old, old);
+                            st_hint(out + l, na, keep);
+                            const float ch2 = na - old;
+                            d2 = fmaf(ch2, ch2, d2);
+                            dd = fmaf(na, na, dd);
+                        }
+                    }
+                    // the warp's reads of the stage are done: release it
+                    __syncwarp();
+                    if (lane == 0) mbar_arrive(&empty[s]);
+                    if (check) {
+                        // this warp's sums for the chunk (the model's
+                        // decision adds them in a fixed order)
+                        double a = d2, e = dd;
+#pragma unroll
+                        for (int o = 16; o > 0; o >>= 1) {
+                            a = a + __shfl_down_sync(0xffffffffu, a, o);
+                            e = e + __shfl_down_sync(0xffffffffu, e, o);
+                        }
+                        if (lane == 0) A.cpart[(2 * q + col) * 4 + (warp & 3)] = make_double2(a, e);
+                    }
+                }
+            }
+            uses += (unsigned)mine;
+            fence_proxy_async();
+            __syncthreads();
+            if (*err) { ok = false; break; }
+            ok = grid_sync(A.bar, nb);
+        }
+        if (!ok) break;
+        if (check || last) {
+            for (int it = (int)b; it < A.nitems; it += (int)nb) {
+                const FusedItem& I = A.items[it];
+                double s1 = 0.0, s3 = 0.0;
+                if (check)
+                    for (long long k = tid; k < I.nchunks; k += blockDim.x) {
+                        const double2* pk = A.cpart + 8 * (I.cfirst + k);   // 2 colours x 4 warps
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            const double2 pj = __ldcg(pk + j);
+                            s1 = s1 + pj.x;
+                            s3 = s3 + pj.y;
+                        }
+                    }
+                s1 = block_sum<kTmaThreads>(s1, sh);
+                s3 = block_sum<kTmaThreads>(s3, sh);
+                if (tid == 0) fused_decide(I, g, num_it, check, s1, s3, A.any_event);
+                __syncthreads();
+            }
+            ok = grid_sync(A.bar, nb);
+            if (ok && *(volatile int*)A.any_event) break;
+        }
+    }
+    if (!ok && producer && lane == 0) {
+        // the last copies issued into each stage land before the block's
+        // shared memory is released (bounded waits, flag ignored)
+        atomicExch(&A.bar->error, 1);
+        const unsigned first = issued > (unsigned)kTmaStages ? issued - kTmaStages : 0u;
+        for (unsigned v = first; v < issued; ++v)
+            mbar_wait_bounded(&full[v % kTmaStages], (v / kTmaStages) & 1u);
+    }
+    if (!ok && b == 0 && tid == 0)
+        for (int it = 0; it < A.nitems; ++it) A.items[it].c.st->event = EV_ERROR;
+}
+
+__global__ void fused_gather_kernel(const FusedItem* items, int n, DcState* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = *items[i].c.st;
+}
+
+constexpr size_t kFusedMaxSmem = 200 * 1024;
+
+// bytes of the fused form's batch workspace for n models of `cells` cells in all
+static size_t fused_ws_bytes(int n, long long cells) {
+    const size_t nch = (size_t)(cells / kTmaChunk) + (size_t)n + 1;
+    return align256(sizeof(FusedItem) * n) + align256(sizeof(FusedChunk) * nch) +
+           align256(sizeof(double2) * 8 * nch) + align256(sizeof(DcState) * n) + 256 +
+           align256(sizeof(GridBarrier)) + 256;
+}
+
+template <class Form>
+static int run_fused(std::vector<BatchItem<Form>>& v, void* d_ws, size_t ws_bytes, cudaStream_t stream) {
+    const int n = (int)v.size();
+    long long cells = 0;
+    int Hmax = 0;
+    for (auto& it : v) {
+        cells += (long long)it.c.L.nx * it.c.L.ny * it.c.L.nz;
+        Hmax = it.c.L.H > Hmax ? it.c.L.H : Hmax;
+    }
+    if (fused_ws_bytes(n, cells) > ws_bytes) return TSE_ERR_WORKSPACE;
+    const TmaStage T = tma_stage(Hmax);
+    const size_t smem = (size_t)kTmaStages * T.bytes;
+    if (smem > kFusedMaxSmem) return TSE_ERR_ARG;
+    // carve the batch workspace
+    const size_t nch_max = (size_t)(cells / kTmaChunk) + (size_t)n + 1;
+    char* p = (char*)d_ws;
+    FusedItem* d_items = (FusedItem*)p;
+    p += align256(sizeof(FusedItem) * n);
+    FusedChunk* d_chunks = (FusedChunk*)p;
+    p += align256(sizeof(FusedChunk) * nch_max);
+    double2* d_cpart = (double2*)p;
+    p += align256(sizeof(double2) * 8 * nch_max);
+    DcState* d_states = (DcState*)p;
+    p += align256(sizeof(DcState) * n);
+    int* d_any = (int*)p;
+    p += 256;
+    GridBarrier* d_bar = (GridBarrier*)p;
+
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaFuncSetAttribute(fused_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)kFusedMaxSmem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fused_sweep_kernel, kTmaThreads, smem) !=
+            cudaSuccess ||
+        per_sm < 1)
+        return TSE_ERR_LAUNCH;
+
+    // every model: state, scaled records, first residual
+    for (auto& it : v) {
+        int rc = dc_begin(it.F, it.c, it.dt, stream);
+        if (rc == TSE_OK) rc = dc_residual(it.F, it.c, stream);
+        if (rc != TSE_OK) return rc;
+    }
+    std::vector<int> active(n), inner(n, 0);
+    for (int i = 0; i < n; ++i) active[i] = i;
+    std::vector<DcState> st(n);
+    for (int i = 0; i < n; ++i) {
+        memset(&st[i], 0, sizeof(DcState));
+        st[i].dt = v[i].dt;
+    }
+    int num_it = 0;
+    int rc = TSE_OK;
+    std::vector<FusedItem> hitems;
+    std::vector<FusedChunk> hchunks;
+    std::vector<DcState> got;
+    while (!active.empty()) {
+        // the nearest cycle end or dt halving among the active models
+        int g_max = 1 << 30;
+        for (int i : active) {
+            const DcCtl& c = v[i].c;
+            int lim = c.cycle - inner[i];
+            const int h = c.max_it - st[i].num_sub_it;
+            lim = h < lim ? h : lim;
+            if (st[i].dt <= c.min_dt) lim = 1;
+            g_max = lim < g_max ? lim : g_max;
+        }
+        if (g_max < 1) g_max = 1;
+        hitems.clear();
+        hchunks.clear();
+        for (int k = 0; k < (int)active.size(); ++k) {
+            const int i = active[k];
+            FusedItem I;
+            memset(&I, 0, sizeof(I));
+            I.c = v[i].c;
+            I.cfirst = (long long)hchunks.size();
+            const long long nc = (v[i].c.L.Nc + kTmaChunk - 1) / kTmaChunk;
+            I.nchunks = nc;
+            I.inner = inner[i];
+            for (long long q = 0; q < nc; ++q) hchunks.push_back(FusedChunk{q * kTmaChunk, k, 0});
+            hitems.push_back(I);
+        }
+        const int na = (int)hitems.size();
+        const long long nch = (long long)hchunks.size();
+        FusedArgs A;
+        A.items = d_items;
+        A.nitems = na;
+        A.chunks = d_chunks;
+        A.nchunks = nch;
+        A.cpart = d_cpart;
+        A.any_event = d_any;
+        A.bar = d_bar;
+        A.g_max = g_max;
+        A.num_it0 = num_it;
+        A.pressure_schedule = v[0].c.pressure_schedule;
+        long long nb = (long long)sms * per_sm;
+        if (nb > nch) nb = nch;
+        if (nb > kMaxBlocks) nb = kMaxBlocks;
+        // pageable sources: staged before the calls return
+        if (cudaMemcpyAsync(d_items, hitems.data(), sizeof(FusedItem) * na, cudaMemcpyHostToDevice,
+                            stream) != cudaSuccess ||
+            cudaMemcpyAsync(d_chunks, hchunks.data(), sizeof(FusedChunk) * nch, cudaMemcpyHostToDevice,
+                            stream) != cudaSuccess ||
+            cudaMemsetAsync(d_any, 0, sizeof(int), stream) != cudaSuccess ||
+            cudaMemsetAsync(d_bar, 0, sizeof(GridBarrier), stream) != cudaSuccess) {
+            rc = TSE_ERR_LAUNCH;
+            break;
+        }
+        void* args[] = {(void*)&A, (void*)&T};
+        if (cudaLaunchCooperativeKernel((const void*)fused_sweep_kernel, dim3((unsigned)nb),
+                                        dim3(kTmaThreads), args, smem, stream) != cudaSuccess) {
+            rc = TSE_ERR_LAUNCH;
+            break;
+        }
+        fused_gather_kernel<<<(na + 127) / 128, 128, 0, stream>>>(d_items, na, d_states);
+        got.resize(na);
+        if (cudaGetLastError() != cudaSuccess ||
+            cudaMemcpyAsync(got.data(), d_states, sizeof(DcState) * na, cudaMemcpyDeviceToHost,
+                            stream) != cudaSuccess ||
+            cudaStreamSynchronize(stream) != cudaSuccess) {
+            rc = TSE_ERR_LAUNCH;
+            break;
+        }
+        const int ran = got[0].num_it - num_it;
+        num_it = got[0].num_it;
+        std::vector<int> next;
+        bool failed = false;
+        for (int k = 0; k < na; ++k) {
+            const int i = active[k];
+            st[i] = got[k];
+            inner[i] += ran;
+            const int ev = got[k].event;
+            int r = TSE_OK;
+            bool done = false;
+            switch (ev) {
+                case EV_NONE: break;
+                case EV_CONVERGED:
+                case EV_STOP: r = dc_apply(v[i].c, stream); done = true; break;
+                case EV_REFRESH:
+                case EV_CYCLE_END:
+                    r = dc_apply(v[i].c, stream);
+                    if (r == TSE_OK) r = dc_residual(v[i].F, v[i].c, stream);
+                    inner[i] = 0;
+                    break;
+                case EV_HALVE:
+                    r = dc_halve(v[i].F, v[i].c, stream);
+                    if (r == TSE_OK) r = dc_residual(v[i].F, v[i].c, stream);
+                    inner[i] = 0;
+                    break;
+                case EV_STOP_HALVED: r = dc_halve(v[i].F, v[i].c, stream); done = true; break;
+                default: failed = true; done = true; break;   // EV_ERROR: reported per model
+            }
+            if (r != TSE_OK) rc = r;
+            if (!done) next.push_back(i);
+        }
+        if (rc != TSE_OK) break;
+        if (failed) {
+            active.clear();
+            break;
+        }
+        active.swap(next);
+    }
+    // status records and results of every model (a failed launch leaves
+    // the models' state records as they were)
+    for (auto& it : v) {
+        const int r = dc_finish(it.c, it.status, it.X_out, stream);
+        if (rc == TSE_OK) rc = r;
+    }
+    return rc;
+}
+
 }  // namespace tse
 
 using namespace tse;
 
-extern "C" size_t tse_batch_workspace_bytes(int32_t n) {
+extern "C" size_t tse_batch_workspace_bytes(int32_t n, int64_t total_cells) {
+    if (n < 1) n = 1;
+    if (total_cells < 0) total_cells = 0;
     const size_t a = sizeof(BatchItem<PressureForm>), b = sizeof(BatchItem<TransportForm>);
-    return align256((a > b ? a : b) * (size_t)(n > 0 ? n : 1)) + 256;
+    const size_t cluster = align256((a > b ? a : b) * (size_t)n) + 256;
+    const size_t fused = fused_ws_bytes(n, total_cells);
+    return cluster > fused ? cluster : fused;
 }
 
 extern "C" int32_t tse_compute_P_dc_batch(const TseBatchPressure* items, int32_t n,
@@ -361,7 +806,8 @@ extern "C" int32_t tse_compute_P_dc_batch(const TseBatchPressure* items, int32_t
         v[i].X_out = a->P;
         v[i].cells = 2 * S.L.Nc;
     }
-    return launch_batch(v, opts, d_batch_ws, batch_ws_bytes, stream);
+    if (opts && opts->max_blocks > 0) return launch_batch(v, opts, d_batch_ws, batch_ws_bytes, stream);
+    return run_fused(v, d_batch_ws, batch_ws_bytes, stream);
 }
 
 extern "C" int32_t tse_compute_C_dc_batch(const TseBatchSpecies* items, int32_t n,
@@ -389,7 +835,8 @@ extern "C" int32_t tse_compute_C_dc_batch(const TseBatchSpecies* items, int32_t 
         v[i].X_out = a->C;
         v[i].cells = 2 * S.L.Nc;
     }
-    return launch_batch(v, opts, d_batch_ws, batch_ws_bytes, stream);
+    if (opts && opts->max_blocks > 0) return launch_batch(v, opts, d_batch_ws, batch_ws_bytes, stream);
+    return run_fused(v, d_batch_ws, batch_ws_bytes, stream);
 }
 
 extern "C" int32_t tse_compute_T_dc_batch(const TseBatchHeat* items, int32_t n,
@@ -417,5 +864,6 @@ extern "C" int32_t tse_compute_T_dc_batch(const TseBatchHeat* items, int32_t n,
         v[i].X_out = a->T;
         v[i].cells = 2 * S.L.Nc;
     }
-    return launch_batch(v, opts, d_batch_ws, batch_ws_bytes, stream);
+    if (opts && opts->max_blocks > 0) return launch_batch(v, opts, d_batch_ws, batch_ws_bytes, stream);
+    return run_fused(v, d_batch_ws, batch_ws_bytes, stream);
 }

@@ -251,225 +251,7 @@ __global__ void __launch_bounds__(kSweepBlock, kSweepMinBlocks) dc_sweep_kernel(
 }
 
 // ------------------------------------------------ FP32 sweeps, TMA-staged
-// The same iterations as dc_sweep_kernel, with the memory side rebuilt for
-// bytes in flight: the cells of a colour are cut into chunks of kTmaChunk,
-// block b takes chunks b, b + G, ...; for each chunk one thread issues bulk
-// asynchronous copies (cp.async.bulk, completion counted on an mbarrier) of
-// everything the chunk's relaxations read -- the 24-byte coefficient records,
-// r', the flag bytes, the old correction and three windows of the other
-// colour's correction (x+, x-, and one covering y+-, z+-) -- into one of
-// kTmaStages shared-memory stages; the block computes from filled stages
-// while later chunks are in flight, so each SM keeps up to ~190 KB of reads
-// outstanding with no registers held for them.  The per-cell arithmetic is
-// relax()'s, operation for operation, so the corrections are identical to
-// dc_sweep_kernel's; only the grouping of the check sums differs.
-#ifndef TSE_TMA_CHUNK
-#define TSE_TMA_CHUNK 512
-#endif
-#ifndef TSE_TMA_STAGES
-#define TSE_TMA_STAGES 4   // two stages in computation, the rest in flight
-#endif
-#ifndef TSE_TMA_MINB
-#define TSE_TMA_MINB 2
-#endif
-constexpr int kTmaChunk = TSE_TMA_CHUNK;
-constexpr int kTmaStages = TSE_TMA_STAGES;
-static_assert(kTmaChunk % 32 == 0, "chunk: 16-byte copies of every array");
-static_assert(kTmaChunk <= kDcMaxChunk, "windows must stay inside the correction margins");
-
-// byte offsets of one stage's arrays (all multiples of 16)
-struct TmaStage {
-    int rec, rp, msk, dw, wz, wxp, wxm, bytes;
-    int lz, lx;   // window lengths in floats
-};
-
-__host__ __device__ inline TmaStage tma_stage(int H) {
-    TmaStage t;
-    const int C = kTmaChunk;
-    t.rec = 0;
-    t.rp = 24 * C;
-    t.msk = t.rp + 4 * C;
-    t.dw = t.msk + C;
-    t.wz = t.dw + 4 * C;
-    // [m0 - H - 1, m0 + C + H] from a start rounded down by up to 3 floats
-    t.lz = (C + 2 * H + 5 + 3) & ~3;
-    // [m0 +- SX, m0 +- SX + C) from a start rounded down by up to 3 floats
-    t.lx = C + 4;
-    t.wxp = t.wz + 4 * t.lz;
-    t.wxm = t.wxp + 4 * t.lx;
-    t.bytes = (t.wxm + 4 * t.lx + 127) & ~127;
-    return t;
-}
-
-__device__ __forceinline__ unsigned smem_u32(const void* p) {
-    return static_cast<unsigned>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-// the stage's single arrival, adding `bytes` to its transaction count
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-                 "r"(bytes)
-                 : "memory");
-}
-
-// adds `bytes` to the transaction count without arriving
-__device__ __forceinline__ void mbar_add_tx(uint64_t* bar, unsigned bytes) {
-    asm volatile("mbarrier.expect_tx.relaxed.cta.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)),
-                 "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
-    unsigned done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(smem_u32(bar)), "r"(parity)
-        : "memory");
-    return done != 0;
-}
-
-// bulk copy global -> this CTA's shared memory; 16-byte aligned, size % 16 == 0
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
-        ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
-        : "memory");
-}
-
-// L2 eviction priority.  Per iteration the coefficient records, r' and the
-// flags stream ~29 bytes a cell once (far more than L2 holds), while the two
-// correction arrays (8 bytes a cell) are reread by the next phase's windows:
-// the stream is marked evict-first and the corrections evict-last, so the
-// corrections stay in L2 instead of being pushed out by the stream.
-#ifndef TSE_TMA_HINTS
-#define TSE_TMA_HINTS 1
-#endif
-__device__ __forceinline__ uint64_t l2_evict_first() {
-    uint64_t p;
-    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
-    return p;
-}
-__device__ __forceinline__ uint64_t l2_evict_last() {
-    uint64_t p;
-    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
-    return p;
-}
-
-__device__ __forceinline__ void bulk_g2s_hint(void* dst, const void* src, unsigned bytes, uint64_t* bar,
-                                              uint64_t policy) {
-#if TSE_TMA_HINTS
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
-        " [%0], [%1], %2, [%3], %4;"
-        ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
-        : "memory");
-#else
-    bulk_g2s(dst, src, bytes, bar);
-#endif
-}
-
-__device__ __forceinline__ void st_hint(float* p, float v, uint64_t policy) {
-#if TSE_TMA_HINTS
-    asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(p), "f"(v), "l"(policy) : "memory");
-#else
-    *p = v;
-#endif
-}
-
-// orders this thread's generic-proxy global accesses with async-proxy copies
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async;" ::: "memory"); }
-
-// bounded wait for a stage; false after kBarrierTimeoutNs
-__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, unsigned parity) {
-    if (mbar_try_wait(bar, parity)) return true;
-    const uint64_t t0 = globaltimer();
-    unsigned spins = 0;
-    while (!mbar_try_wait(bar, parity)) {
-        if ((++spins & 63u) == 0u && globaltimer() - t0 > kBarrierTimeoutNs) return false;
-    }
-    return true;
-}
-
-// Chunk q of the colour being swept, in two parts.  The first part (records,
-// r', flags, the chunk's own old correction) depends on nothing another block
-// writes during the launch -- the old correction of a chunk is written only
-// by the block that owns the chunk -- so it may be issued before the grid
-// barrier that ends the previous phase; it adds its bytes to the stage's
-// transaction count without arriving.  The second part (the three windows of
-// the other colour, which other blocks have just written) is issued after the
-// barrier and carries the stage's single arrival.
-__device__ __forceinline__ void tma_issue_own(const DcCtl& c, const TmaStage& T, unsigned char* stage,
-                                              uint64_t* bar, const float* Kc, const float* dw,
-                                              const uint8_t* msk, long long m0, long long cnt) {
-    const long long N = c.Ncal;
-    const unsigned b_rec = (unsigned)(24 * cnt), b_rp = (unsigned)(4 * cnt), b_msk = (unsigned)cnt,
-                   b_dw = (unsigned)(4 * cnt);
-    const uint64_t first = l2_evict_first(), last = l2_evict_last();
-    mbar_add_tx(bar, b_rec + b_rp + b_msk + b_dw);
-    bulk_g2s_hint(stage + T.rec, Kc + 6 * m0, b_rec, bar, first);
-    bulk_g2s_hint(stage + T.rp, Kc + 6 * N + m0, b_rp, bar, first);
-    bulk_g2s_hint(stage + T.msk, msk + m0, b_msk, bar, first);
-    bulk_g2s_hint(stage + T.dw, dw + m0, b_dw, bar, last);
-    (void)N;
-}
-
-__device__ __forceinline__ void tma_issue_windows(const DcCtl& c, const TmaStage& T, unsigned char* stage,
-                                                  uint64_t* bar, const float* dq, long long m0) {
-    const long long SX = c.L.SX;
-    const int H = c.L.H;
-    const long long zs = (m0 - H - 1) & ~3LL;
-    const long long xps = (m0 + SX) & ~3LL;
-    const long long xms = (m0 - SX) & ~3LL;
-    const unsigned b_z = (unsigned)(4 * T.lz), b_x = (unsigned)(4 * T.lx);
-    const uint64_t last = l2_evict_last();
-    mbar_expect_tx(bar, b_z + 2 * b_x);
-    bulk_g2s_hint(stage + T.wz, dq + zs, b_z, bar, last);
-    bulk_g2s_hint(stage + T.wxp, dq + xps, b_x, bar, last);
-    bulk_g2s_hint(stage + T.wxm, dq + xms, b_x, bar, last);
-}
-
-// Roles: warps 0-7 consume, in two groups of four warps; group g computes the
-// block's chunks i = g, g + 2, ..., so two chunks are in computation at once
-// and neither waits for the other.  Warp 8 produces: its lane 0 issues the
-// copies of chunk i into stage i % kTmaStages as soon as the consumers of
-// chunk i - kTmaStages have released that stage (`empty` barrier, one arrival
-// per consumer warp).  Consumers wait on the stage's `full` barrier (the
-// copies' byte count).  Only the colour phases end in block- and grid-wide
-// barriers.  Every wait is bounded; a wait that runs out raises a block flag
-// that ends every other wait of the block, and the kernel leaves with
-// EV_ERROR after the copies still in flight have landed (again bounded).
-constexpr int kTmaConsumers = 256;                    // 8 warps, two groups of 4
-constexpr int kTmaGroup = kTmaConsumers / 2;
-constexpr int kTmaThreads = kTmaConsumers + 32;       // + one producer warp
-constexpr int kTmaCellsPerThread = kTmaChunk / kTmaGroup;
-static_assert(kTmaChunk % kTmaGroup == 0, "whole cells per consumer thread");
-
-// wait for a phase of `bar`; gives up (false) when the block's error flag is
-// raised or after kBarrierTimeoutNs, raising the flag
-__device__ __forceinline__ bool mbar_wait_flag(uint64_t* bar, unsigned parity, volatile int* err) {
-    if (mbar_try_wait(bar, parity)) return true;
-    const uint64_t t0 = globaltimer();
-    unsigned spins = 0;
-    while (!mbar_try_wait(bar, parity)) {
-        if (*err) return false;
-        if ((++spins & 63u) == 0u && globaltimer() - t0 > kBarrierTimeoutNs) {
-            *err = 1;
-            return false;
-        }
-    }
-    return true;
-}
-
+// (the staging pieces are in tse_dc.cuh)
 __global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) dc_sweep_tma_kernel(DcCtl c, TmaStage T) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t full[kTmaStages];
@@ -543,7 +325,12 @@ __global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) dc_sweep_tma_kernel
                 for (long long i = group; i < mine; i += 2) {
                     const unsigned u = uses + (unsigned)i;
                     const unsigned s = u % kTmaStages;
-                    if (!mbar_wait_flag(&full[s], (u / kTmaStages) & 1u, err)) break;
+                    // warp-uniform: lane 0 waits, the warp follows its outcome,
+                    // then every lane observes the completed phase (acquire)
+                    int okw = 1;
+                    if (lane == 0) okw = mbar_wait_flag(&full[s], (u / kTmaStages) & 1u, err);
+                    if (!__shfl_sync(0xffffffffu, okw, 0)) break;
+                    mbar_try_wait(&full[s], (u / kTmaStages) & 1u);
                     const unsigned char* stg = smem + (size_t)s * T.bytes;
                     const long long m0 = (b + i * nb) * C;
                     const int nval = (int)((Nc - m0) < C ? (Nc - m0) : C);
@@ -857,6 +644,62 @@ static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, 
     if (cudaGetLastError() != cudaSuccess) return TSE_ERR_LAUNCH;
     return launch_unpack(X_out, c.X[0], c.X[1], S.L, stream);
 }
+
+// ------------------------------------------- per-model steps, for batches
+// The steps run_dc takes for one model, for drivers that interleave many
+// models (tse_batch.cu): start (state record, zero margins, scaled records),
+// residual (r', d = 0, x^2), halving (reset + new R terms + rescale), x += d,
+// and finish (status record + natural-layout result).
+template <class Form>
+int dc_begin(const Form& F, const DcCtl& c, double dt, cudaStream_t stream) {
+    DcState init;
+    memset(&init, 0, sizeof(init));
+    init.dt = dt;
+    init.diff = 1e100;
+    float* dbase = c.D[0] - dc_margin(c.L);
+    const long long dlen = dc_delta_len(c.L, c.Ncal);
+    if (cudaMemsetAsync(dbase, 0, (size_t)2 * dlen * sizeof(float), stream) != cudaSuccess ||
+        cudaMemcpyAsync(c.st, &init, sizeof(DcState), cudaMemcpyHostToDevice, stream) != cudaSuccess)
+        return TSE_ERR_LAUNCH;
+    const unsigned g = (unsigned)((2 * c.L.Nc + kBlock - 1) / kBlock);
+    dc_scale_kernel<<<g, kBlock, 0, stream>>>(F, c);
+    return cudaGetLastError() == cudaSuccess ? TSE_OK : TSE_ERR_LAUNCH;
+}
+
+template <class Form>
+int dc_residual(const Form& F, const DcCtl& c, cudaStream_t stream) {
+    const long long cells2 = 2 * c.L.Nc;
+    const unsigned rb = (unsigned)std::min<long long>(kResBlocks, (cells2 + kBlock - 1) / kBlock);
+    dc_residual_kernel<<<rb, kBlock, 0, stream>>>(F, c);
+    dc_x2_kernel<<<1, kBlock, 0, stream>>>(c, (int)rb);
+    return cudaGetLastError() == cudaSuccess ? TSE_OK : TSE_ERR_LAUNCH;
+}
+
+template <class Form>
+int dc_halve(const Form& F, const DcCtl& c, cudaStream_t stream) {
+    const unsigned g = (unsigned)((2 * c.L.Nc + kBlock - 1) / kBlock);
+    dc_halve_kernel<<<g, kBlock, 0, stream>>>(F, c);
+    return cudaGetLastError() == cudaSuccess ? TSE_OK : TSE_ERR_LAUNCH;
+}
+
+int dc_apply(const DcCtl& c, cudaStream_t stream) {
+    const unsigned g = (unsigned)((2 * c.L.Nc + kBlock - 1) / kBlock);
+    dc_apply_kernel<<<g, kBlock, 0, stream>>>(c);
+    return cudaGetLastError() == cudaSuccess ? TSE_OK : TSE_ERR_LAUNCH;
+}
+
+int dc_finish(const DcCtl& c, TseSolveStatus* d_status, double* X_out, cudaStream_t stream) {
+    dc_status_kernel<<<1, 1, 0, stream>>>(c.st, d_status);
+    if (cudaGetLastError() != cudaSuccess) return TSE_ERR_LAUNCH;
+    return launch_unpack(X_out, c.X[0], c.X[1], c.L, stream);
+}
+
+template int dc_begin<PressureForm>(const PressureForm&, const DcCtl&, double, cudaStream_t);
+template int dc_begin<TransportForm>(const TransportForm&, const DcCtl&, double, cudaStream_t);
+template int dc_residual<PressureForm>(const PressureForm&, const DcCtl&, cudaStream_t);
+template int dc_residual<TransportForm>(const TransportForm&, const DcCtl&, cudaStream_t);
+template int dc_halve<PressureForm>(const PressureForm&, const DcCtl&, cudaStream_t);
+template int dc_halve<TransportForm>(const TransportForm&, const DcCtl&, cudaStream_t);
 
 }  // namespace tse
 

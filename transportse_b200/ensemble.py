@@ -43,7 +43,7 @@ from .batch import BatchGate
 from .driver import Simulation
 
 # resident cooperative blocks per SM of the mixed-precision sweep kernel
-SWEEP_BLOCKS_PER_SM = 5
+SWEEP_BLOCKS_PER_SM = 2   # the staged sweep kernel's residency (dc_sweep_tma_kernel)
 
 
 def state_bytes(config, precision="fp32dc"):
@@ -119,12 +119,10 @@ def block_cap(device, concurrency):
     return max(8, (sms * SWEEP_BLOCKS_PER_SM) // max(1, concurrency))
 
 
-def run_model(config, steps, device, precision, max_blocks, dc_cycle=None, keep=("P", "C", "T"),
-              gate=None, cluster_cells=0, cluster_size=0):
-    """Run one model on the calling thread's current stream; returns results.
-    With ``gate`` its mixed-precision solves are batched through it; else a
-    grid of at most ``cluster_cells`` cells solves in single-cluster launches
-    (``cluster_size`` CTAs) on this stream."""
+def build_model(config, device, precision, max_blocks, dc_cycle=None, cluster_cells=0,
+                cluster_size=0):
+    """Set up one model (device state, workspace, initial EOS) on the calling
+    thread's current stream."""
     sim = Simulation(config, device=device, precision=precision)
     sim.M.max_blocks = int(max_blocks)
     sim.M.cluster_cells = int(cluster_cells)
@@ -132,13 +130,22 @@ def run_model(config, steps, device, precision, max_blocks, dc_cycle=None, keep=
         sim.M.cluster_size = int(cluster_size)
     if dc_cycle:
         sim.M.dc_cycle = int(dc_cycle)
+    return sim
+
+
+def step_model(sim, steps, keep=("P", "C", "T"), gate=None, joined=False):
+    """Advance a built model by ``steps`` steps; returns its results.  With
+    ``gate`` its mixed-precision solves are batched through it (``joined``:
+    the caller has already counted this thread as a member)."""
     if gate is not None:
-        with gate.member():
-            sim.M.batch_gate = gate
-            try:
-                sim.run(max_steps=steps)
-            finally:
-                sim.M.batch_gate = None
+        if not joined:
+            gate.join()
+        sim.M.batch_gate = gate
+        try:
+            sim.run(max_steps=steps)
+        finally:
+            sim.M.batch_gate = None
+            gate.leave()
     else:
         sim.run(max_steps=steps)
     out = {k: sim.field(k) for k in keep}
@@ -147,6 +154,16 @@ def run_model(config, steps, device, precision, max_blocks, dc_cycle=None, keep=
     out["t_sim"] = sim.t_sim
     out["iterations"] = dict(sim.counters)
     return out
+
+
+def run_model(config, steps, device, precision, max_blocks, dc_cycle=None, keep=("P", "C", "T"),
+              gate=None, cluster_cells=0, cluster_size=0):
+    """Run one model on the calling thread's current stream; returns results.
+    With ``gate`` its mixed-precision solves are batched through it; else a
+    grid of at most ``cluster_cells`` cells solves in single-cluster launches
+    (``cluster_size`` CTAs) on this stream."""
+    sim = build_model(config, device, precision, max_blocks, dc_cycle, cluster_cells, cluster_size)
+    return step_model(sim, steps, keep, gate)
 
 
 def autotune(configs, device=None, precision="fp32dc", steps=1, concurrency=(2, 4, 8),
@@ -210,47 +227,125 @@ class Ensemble:
         self.cluster = int(cluster)
         self.gate = BatchGate(self.device, cluster=self.cluster) if self.batched else None
 
-    def run(self, steps, keep=("P", "C", "T")):
-        """Advance every model by ``steps`` time steps; returns (results, stats)."""
-        todo = queue.Queue()
-        for i, cfg in enumerate(self.configs):
-            todo.put((i, cfg))
-        results = [None] * len(self.configs)
+    def run(self, steps, keep=("P", "C", "T"), prebuild=None):
+        """Advance every model by ``steps`` time steps; returns (results, stats).
+
+        prebuild (default: when every model fits the HBM budget at once): set
+        every model up first, then step them, and report the two phases
+        apart (``setup_s``, ``step_s``, ``stepping_cell_updates_per_s``);
+        otherwise models are admitted one by one as memory frees up and only
+        the whole wall time is known.  Batched runs always prebuild."""
+        needs = [state_bytes(cfg, self.precision) for cfg in self.configs]
+        if prebuild is None:
+            prebuild = sum(needs) <= self.budget.total
+        if self.batched and not prebuild:
+            raise MemoryError("batched: every model must be resident at once (%.1f GB needed, "
+                              "budget %.1f GB)" % (sum(needs) / 1e9, self.budget.total / 1e9))
+        n = len(self.configs)
+        results = [None] * n
         errors = []
         t0 = time.perf_counter()
+        setup = None
 
-        def worker():
-            stream = torch.cuda.Stream(device=self.device)
-            while True:
-                try:
-                    i, cfg = todo.get_nowait()
-                except queue.Empty:
-                    return
-                need = state_bytes(cfg, self.precision)
-                self.budget.acquire(need)
-                try:
-                    with torch.cuda.device(self.device), torch.cuda.stream(stream):
-                        results[i] = run_model(cfg, steps, self.device, self.precision,
-                                               self.max_blocks, self.dc_cycle, keep, self.gate,
-                                               self.cluster_cells, self.cluster)
-                        stream.synchronize()
-                except Exception as e:   # reported after all workers stop
-                    errors.append((i, e))
-                finally:
-                    self.budget.release(need)
+        def build_all():
+            sims = [None] * n
+            todo = queue.Queue()
+            for i in range(n):
+                todo.put(i)
 
-        threads = [threading.Thread(target=worker, daemon=True) for _ in range(self.concurrency)]
+            def builder():
+                stream = torch.cuda.Stream(device=self.device)
+                with torch.cuda.device(self.device), torch.cuda.stream(stream):
+                    while True:
+                        try:
+                            i = todo.get_nowait()
+                        except queue.Empty:
+                            break
+                        try:
+                            sims[i] = build_model(self.configs[i], self.device, self.precision,
+                                                  self.max_blocks, self.dc_cycle, self.cluster_cells,
+                                                  self.cluster)
+                        except Exception as e:
+                            errors.append((i, e))
+                    stream.synchronize()
+            ths = [threading.Thread(target=builder, daemon=True) for _ in range(min(8, n))]
+            for th in ths:
+                th.start()
+            for th in ths:
+                th.join()
+            return sims
+
+        if prebuild:
+            sims = build_all()
+            setup = time.perf_counter() - t0
+            if errors:
+                i, e = errors[0]
+                raise RuntimeError("model %d failed: %s" % (i, e)) from e
+            todo = queue.Queue()
+            for i in range(n):
+                todo.put(i)
+            nthreads = n if self.batched else self.concurrency
+            if self.batched:
+                for _ in range(n):
+                    self.gate.join()   # every model is a member before any solves
+
+            def stepper():
+                stream = torch.cuda.Stream(device=self.device)
+                while True:
+                    try:
+                        i = todo.get_nowait()
+                    except queue.Empty:
+                        return
+                    try:
+                        with torch.cuda.device(self.device), torch.cuda.stream(stream):
+                            results[i] = step_model(sims[i], steps, keep, self.gate, joined=True)
+                            stream.synchronize()
+                    except Exception as e:   # reported after all workers stop
+                        errors.append((i, e))
+                    sims[i] = None   # its device memory goes back to the pool
+
+            threads = [threading.Thread(target=stepper, daemon=True) for _ in range(nthreads)]
+        else:
+            todo = queue.Queue()
+            for i, cfg in enumerate(self.configs):
+                todo.put((i, cfg))
+
+            def admitter():
+                stream = torch.cuda.Stream(device=self.device)
+                while True:
+                    try:
+                        i, cfg = todo.get_nowait()
+                    except queue.Empty:
+                        return
+                    self.budget.acquire(needs[i])
+                    try:
+                        with torch.cuda.device(self.device), torch.cuda.stream(stream):
+                            results[i] = run_model(cfg, steps, self.device, self.precision,
+                                                   self.max_blocks, self.dc_cycle, keep, None,
+                                                   self.cluster_cells, self.cluster)
+                            stream.synchronize()
+                    except Exception as e:   # reported after all workers stop
+                        errors.append((i, e))
+                    finally:
+                        self.budget.release(needs[i])
+
+            threads = [threading.Thread(target=admitter, daemon=True) for _ in range(self.concurrency)]
+        t1 = time.perf_counter()
         for th in threads:
             th.start()
         for th in threads:
             th.join()
-        wall = time.perf_counter() - t0
+        t2 = time.perf_counter()
+        wall = t2 - t0
         if errors:
             i, e = errors[0]
             raise RuntimeError("model %d failed: %s" % (i, e)) from e
         updates = sum(r["cell_updates"] for r in results)
+        step_s = (t2 - t1) if prebuild else None
         return results, {"wall_s": wall, "cell_updates": updates,
                          "cell_updates_per_s": updates / wall if wall > 0 else 0.0,
+                         "setup_s": setup, "step_s": step_s,
+                         "stepping_cell_updates_per_s": (updates / step_s) if step_s else None,
                          "models": len(results), "concurrency": self.concurrency,
                          "max_blocks": self.max_blocks, "batched": self.batched,
                          "cluster_cells": self.cluster_cells,

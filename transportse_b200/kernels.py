@@ -134,7 +134,7 @@ class Model:
         L = N.lib()
         bws = self.__dict__.get("_cluster_ws")
         if bws is None:
-            bws = self._cluster_ws = torch.empty(int(L.tse_batch_workspace_bytes(1)),
+            bws = self._cluster_ws = torch.empty(int(L.tse_batch_workspace_bytes(1, self.n)),
                                                  dtype=torch.uint8, device=self.device)
         Item = N.BATCH_ITEM[name]
         items = (Item * 1)(Item(ct.pointer(self.grid), ct.pointer(args_struct),
