@@ -45,6 +45,15 @@ constexpr int kSweepBlock = TSE_SWEEP_BLOCK;
 #ifndef TSE_SWEEP_CHUNKED
 #define TSE_SWEEP_CHUNKED 0   // 1: contiguous chunks with neighbour-only phase sync
 #endif
+#ifndef TSE_TMA_ROUNDSYNC
+#define TSE_TMA_ROUNDSYNC 0  // 1: colour phases ordered per round of chunks, device-wide
+                             // barrier only before a check's sums (measured 2.7x slower:
+                             // the per-chunk proxy fence and GPU-scope release sit on
+                             // the critical path)
+#endif
+#ifndef TSE_TMA_PREFETCH
+#define TSE_TMA_PREFETCH 1   // 1: a phase's own parts are copied before its grid barrier
+#endif
 constexpr int kResBlocks = 2048;   // fixed grid of the residual kernel (deterministic sums)
 
 // ------------------------------------------------------------ FP64 kernels
@@ -252,6 +261,79 @@ __global__ void __launch_bounds__(kSweepBlock, kSweepMinBlocks) dc_sweep_kernel(
 
 // ------------------------------------------------ FP32 sweeps, TMA-staged
 // (the staging pieces are in tse_dc.cuh)
+// Rounds.  Chunk q = r nb + b is block b's chunk of round r, so a round is a
+// contiguous range of nb chunks, and a chunk's windows reach at most
+// SX + H + 16 cells beyond it: rounds r - delta .. r + delta.  When the
+// consumers of a chunk have written it and released its stage, the producer
+// (which waits for that release anyway) adds 1 to the round's counter
+// (release, GPU scope); before copying a chunk's windows in the next colour
+// phase it makes sure those rounds of the previous phase are complete
+// (acquire, bounded) -- every write it reads is then done, and so is every
+// read of the cells it is about to overwrite.  At a phase end the producer
+// posts all of the phase's chunks, so no round waits for a later phase.  The
+// device-wide barrier remains only before a check's sums.
+__device__ __forceinline__ void red_release_add(unsigned* p, unsigned v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// producer: advance `ready` (every round <= ready has completed `phases`
+// phases, one post per chunk) until it reaches `need`; false on the block's
+// error flag or after kBarrierTimeoutNs, raising the flag
+__device__ __forceinline__ bool rounds_ready(const unsigned* cnt, long long& ready, long long need,
+                                             long long nch, unsigned nb, unsigned phases,
+                                             volatile int* err) {
+    uint64_t t0 = 0;
+    unsigned spins = 0;
+    while (ready < need) {
+        const long long q = ready + 1;
+        const long long in_round = (nch - q * nb) < (long long)nb ? (nch - q * nb) : (long long)nb;
+        if (ld_acquire_u32(cnt + q) >= phases * (unsigned)in_round) {
+            ready = q;
+            continue;
+        }
+        if (*err) return false;
+        if (t0 == 0) t0 = globaltimer();
+        if ((++spins & 63u) == 0u && globaltimer() - t0 > kBarrierTimeoutNs) {
+            *err = 1;
+            return false;
+        }
+        __nanosleep(32);
+    }
+    return true;
+}
+
+// Device-wide barrier of the staged sweep: each block adds 1 to a counter
+// that is zeroed before the launch and never reset in it (release, no value
+// returned), and barrier k of the launch is passed once the counter reaches
+// k * nb (acquire).  No returning atomic, reset or generation flip sits
+// between the last arrival and the waiters' release.  Bounded like
+// grid_sync: on timeout (or another block's error) the error flag is raised
+// and false returned.
+__device__ __forceinline__ bool count_sync(unsigned* counter, unsigned target, GridBarrier* bar) {
+    __syncthreads();
+    __shared__ int s_ok;
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        red_release_add(counter, 1u);
+        if (ld_acquire_u32(counter) < target) {
+            const uint64_t t0 = globaltimer();
+            unsigned spins = 0;
+            while (ld_acquire_u32(counter) < target) {
+                if (*(volatile int*)&bar->error) { ok = 0; break; }
+                if ((++spins & 255u) == 0u && globaltimer() - t0 > kBarrierTimeoutNs) {
+                    atomicExch(&bar->error, 1);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
 __global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) dc_sweep_tma_kernel(DcCtl c, TmaStage T) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t full[kTmaStages];
@@ -268,6 +350,16 @@ __global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) dc_sweep_tma_kernel
     const int H = c.L.H;
     const long long nch = (Nc + C - 1) / C;
     const long long mine = nch > (long long)b ? (nch - 1 - b) / nb + 1 : 0;   // chunks of this block
+    const long long R = (nch + nb - 1) / nb;                                   // rounds
+    const long long delta = (SX + H + 16 + (long long)nb * C - 1) / ((long long)nb * C);
+    long long ready = -1;        // producer: rounds known complete for the previous phase
+    unsigned* rounds = c.prog;   // per round: chunks posted, zeroed before the launch
+    unsigned* bar_count = c.prog + (kMaxBlocks - 1);   // count_sync's counter (zeroed too)
+    unsigned bars = 0;           // device-wide barriers passed in this launch
+    unsigned phase = 0;          // colour phases completed in this launch
+    unsigned posted = 0;         // producer: uses posted to their round
+    int stage_round[kTmaStages]; // producer: round of each stage's latest use
+    for (int q = 0; q < kTmaStages; ++q) stage_round[q] = q;
     const bool leader = (b == 0 && tid == 0);
     const float sor = c.sor;
     const uint64_t keep = l2_evict_last();
@@ -290,6 +382,20 @@ __global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) dc_sweep_tma_kernel
     __syncthreads();
     unsigned uses = 0;      // chunks this block has consumed, over all colour phases
     unsigned issued = 0;    // producer: chunks issued, over all colour phases
+    // producer: chunks of the coming phase whose own parts are already in flight
+    long long primed = 0;
+    const long long pro = mine < kTmaStages ? mine : kTmaStages;
+#if TSE_TMA_PREFETCH
+    if (producer && lane == 0) {
+        for (long long j = 0; j < pro; ++j) {
+            const long long m0 = (b + j * nb) * C;
+            const long long cnt = (N - m0) < C ? (N - m0) : C;
+            tma_issue_own(c, T, smem + (size_t)j * T.bytes, &full[j], c.K[0], c.D[0], c.mask[0], m0,
+                          cnt);
+        }
+        primed = pro;
+    }
+#endif
 
     for (int inner = 0; inner < c.cycle; ++inner) {
         num_it += 1;
@@ -308,17 +414,73 @@ __global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) dc_sweep_tma_kernel
                     // the other colour was written (generic stores) before
                     // the grid barrier; the copies read it through the async proxy
                     fence_proxy_async();
+                    bool pok = true;
                     for (long long i = 0; i < mine; ++i, ++issued) {
                         const unsigned s = issued % kTmaStages;
-                        if (issued >= (unsigned)kTmaStages &&
-                            !mbar_wait_flag(&empty[s], (issued / kTmaStages - 1) & 1u, err))
-                            break;
                         const long long m0 = (b + i * nb) * C;
-                        const long long cnt = (N - m0) < C ? (N - m0) : C;   // % 32 == 0
                         unsigned char* stg = smem + (size_t)s * T.bytes;
-                        tma_issue_own(c, T, stg, &full[s], Kc, dw, msk, m0, cnt);
+                        if (i >= primed) {
+                            if (issued >= (unsigned)kTmaStages &&
+                                !mbar_wait_flag(&empty[s], (issued / kTmaStages - 1) & 1u, err)) {
+                                pok = false;
+                                break;
+                            }
+#if TSE_TMA_ROUNDSYNC
+                            // the stage's previous chunk is written: post it
+                            if (issued >= (unsigned)kTmaStages && posted <= issued - kTmaStages) {
+                                red_release_add(rounds + stage_round[s], 1u);
+                                posted = issued - kTmaStages + 1;
+                            }
+#endif
+                            const long long cnt = (N - m0) < C ? (N - m0) : C;   // % 32 == 0
+                            tma_issue_own(c, T, stg, &full[s], Kc, dw, msk, m0, cnt);
+                        }
+#if TSE_TMA_ROUNDSYNC
+                        if (phase > 0) {
+                            const long long need = i + delta < R - 1 ? i + delta : R - 1;
+                            if (ready < need) {
+                                if (!rounds_ready(rounds, ready, need, nch, nb, phase, err)) {
+                                    pok = false;
+                                    break;
+                                }
+                                fence_proxy_async();
+                            }
+                        }
+                        stage_round[s] = (int)i;
+#endif
                         tma_issue_windows(c, T, stg, &full[s], dq, m0);
                     }
+                    primed = 0;
+#if TSE_TMA_ROUNDSYNC
+                    // post every chunk of this phase once its consumers are done
+                    for (; pok && posted < issued; ++posted) {
+                        const unsigned u = posted;
+                        if (!mbar_wait_flag(&empty[u % kTmaStages], (u / kTmaStages) & 1u, err)) {
+                            pok = false;
+                            break;
+                        }
+                        red_release_add(rounds + stage_round[u % kTmaStages], 1u);
+                    }
+                    ready = -1;   // the next phase checks its rounds afresh
+#endif
+#if TSE_TMA_PREFETCH
+                    // the next phase's own parts (records, r', flags, own
+                    // correction: nothing another block writes) go out as the
+                    // consumers free the stages, before the grid barrier
+                    const int nc = 1 - col;
+                    for (long long j = 0; pok && j < pro; ++j) {
+                        const unsigned v = issued + (unsigned)j;
+                        const unsigned s = v % kTmaStages;
+                        if (v >= (unsigned)kTmaStages &&
+                            !mbar_wait_flag(&empty[s], (v / kTmaStages - 1) & 1u, err))
+                            break;
+                        const long long m0 = (b + j * nb) * C;
+                        const long long cnt = (N - m0) < C ? (N - m0) : C;
+                        tma_issue_own(c, T, smem + (size_t)s * T.bytes, &full[s], c.K[nc], c.D[nc],
+                                      c.mask[nc], m0, cnt);
+                        primed = j + 1;
+                    }
+#endif
                 }
                 __syncwarp();
             } else {
@@ -370,11 +532,17 @@ __global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) dc_sweep_tma_kernel
                         }
                     }
                     // the warp's reads of the stage are done: release it
+#if TSE_TMA_ROUNDSYNC
+                    // and its writes are done: the producer posts them for the
+                    // round once every warp has released the stage
+                    fence_proxy_async();
+#endif
                     __syncwarp();
                     if (lane == 0) mbar_arrive(&empty[s]);
                 }
             }
             uses += (unsigned)mine;
+            phase += 1;
             // this phase's stores are read by the next phase's copies
             fence_proxy_async();
             __syncthreads();
@@ -387,7 +555,13 @@ __global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) dc_sweep_tma_kernel
                     c.partials[4 * b + 2 * (checkno & 1) + 1] = b3;
                 }
             }
-            ok = grid_sync(c.bar, nb);
+#if TSE_TMA_ROUNDSYNC
+            // between phases the rounds order the blocks; a check's sums
+            // need every block
+            if (col == 1 && check) ok = count_sync(bar_count, ++bars * nb, c.bar);
+#else
+            ok = count_sync(bar_count, ++bars * nb, c.bar);
+#endif
         }
         if (!ok) { event = EV_ERROR; break; }
         diff = 1e100;
@@ -433,13 +607,21 @@ __global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) dc_sweep_tma_kernel
         if (halved) { event = EV_HALVE; break; }
         if (refresh) { event = EV_REFRESH; break; }
     }
-    if (event == EV_ERROR && producer && lane == 0) {
-        // the last copies issued into each stage must land before the
-        // block's shared memory is released (bounded waits, flag ignored)
-        atomicExch(&c.bar->error, 1);
-        const unsigned first = issued > (unsigned)kTmaStages ? issued - kTmaStages : 0u;
-        for (unsigned v = first; v < issued; ++v)
+    if (producer && lane == 0) {
+        // every copy this block issued lands before its shared memory is
+        // released (bounded waits, flag ignored): after an error the last
+        // issued use of each stage; primed stages get their missing arrival
+        if (event == EV_ERROR) {
+            atomicExch(&c.bar->error, 1);
+            const unsigned first = issued > (unsigned)kTmaStages ? issued - kTmaStages : 0u;
+            for (unsigned v = first; v < issued; ++v)
+                mbar_wait_bounded(&full[v % kTmaStages], (v / kTmaStages) & 1u);
+        }
+        for (long long j = 0; j < primed; ++j) {
+            const unsigned v = issued + (unsigned)j;
+            mbar_arrive(&full[v % kTmaStages]);
             mbar_wait_bounded(&full[v % kTmaStages], (v / kTmaStages) & 1u);
+        }
     }
     if (leader) {
         st->t = t;
@@ -527,7 +709,11 @@ static int tma_blocks(long long Nc, int cap, size_t smem) {
     if (nb > nch) nb = nch;
     if (nb > kMaxBlocks / 2) nb = kMaxBlocks / 2;
     if (cap > 0 && nb > cap) nb = cap;
-    return nb < 1 ? 1 : (int)nb;
+    if (nb < 1) nb = 1;
+    // one round counter per nb chunks, plus the barrier counter, in the
+    // kMaxBlocks counters of the workspace
+    if ((nch + nb - 1) / nb >= kMaxBlocks) return 0;
+    return (int)nb;
 }
 
 template <class Form>
@@ -586,8 +772,9 @@ static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, 
         dc_x2_kernel<<<1, kBlock, 0, stream>>>(c, (int)rb);
         void* args[] = {(void*)&c};
         void* targs[] = {(void*)&c, (void*)&T};
-        if (TSE_SWEEP_CHUNKED &&
-            cudaMemsetAsync(c.prog, 0, (size_t)nb * sizeof(unsigned), stream) != cudaSuccess) {
+        // chunked sweep: PhaseSync counters; staged sweep: round counters
+        if ((TSE_SWEEP_CHUNKED || nb_tma > 0) &&
+            cudaMemsetAsync(c.prog, 0, (size_t)kMaxBlocks * sizeof(unsigned), stream) != cudaSuccess) {
             rc = TSE_ERR_LAUNCH;
             break;
         }
