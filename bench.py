@@ -45,7 +45,7 @@ ALG_BYTES = {"fp64": 57, "fp32dc": 29}
 # dram__bytes_write.sum of one 64-iteration launch on the 192x192x128
 # reservoir, divided by its cell-updates; summaries under profiles/), scaled
 # to a launch of the benchmark by its cell-updates
-TRAFFIC_BYTES = {"fp32dc": 28.7, "fp64": 114.4}
+TRAFFIC_BYTES = {"fp32dc": 28.8, "fp64": 114.4}
 DEFAULT_SHAPE = (256, 256, 128)
 
 

@@ -449,6 +449,7 @@ __global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) fused_sweep_kernel(
     }
     __syncthreads();
     unsigned uses = 0, issued = 0;
+    unsigned bars = 0;   // device-wide barriers passed (A.bar->count, zeroed per launch)
     bool ok = true;
     for (int g = 1; g <= A.g_max && ok; ++g) {
         const int num_it = A.num_it0 + g;
@@ -545,7 +546,7 @@ __global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) fused_sweep_kernel(
             fence_proxy_async();
             __syncthreads();
             if (*err) { ok = false; break; }
-            ok = grid_sync(A.bar, nb);
+            ok = count_sync(&A.bar->count, ++bars * nb, A.bar);
         }
         if (!ok) break;
         if (check || last) {
@@ -567,7 +568,7 @@ __global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) fused_sweep_kernel(
                 if (tid == 0) fused_decide(I, g, num_it, check, s1, s3, A.any_event);
                 __syncthreads();
             }
-            ok = grid_sync(A.bar, nb);
+            ok = count_sync(&A.bar->count, ++bars * nb, A.bar);
             if (ok && *(volatile int*)A.any_event) break;
         }
     }
