@@ -73,8 +73,12 @@ def parse_args():
                     help="ensemble, unbatched: models in flight (0 = autotune)")
     ap.add_argument("--cluster", type=int, default=0,
                     help="ensemble/serving, batched: CTAs per model (0 = autotune / 8)")
-    ap.add_argument("--unbatched", action="store_true",
-                    help="ensemble/serving: one solve launch per model instead of batched launches")
+    ap.add_argument("--batched", action="store_true",
+                    help="ensemble: lock-step batched solves (one launch per solve kind) instead "
+                         "of concurrent per-model streams (the default)")
+    ap.add_argument("--streams", action="store_true",
+                    help="serving: concurrent per-slot streams instead of batched solves "
+                         "(the default)")
     ap.add_argument("--requests", type=int, default=40, help="serving: requests")
     ap.add_argument("--rate", type=float, default=20.0, help="serving: arrivals per second")
     ap.add_argument("--slots", type=int, default=8, help="serving: concurrent models")
@@ -94,15 +98,10 @@ def bench_ensemble(a):
     nmax = a.n_max or 128
     cfgs = [workloads.ensemble_member(seed=1000 + i, n_max=nmax) for i in range(a.models)]
     tune = None
-    batched = not a.unbatched
+    batched = a.batched
     conc = cyc = cl = None
     if batched:
-        if a.cluster <= 0:
-            tune = autotune(cfgs[:16], device=dev, steps=1, batched=True, clusters=(4, 8, 16),
-                            cycles=(128,))
-            cl = tune["cluster"]
-        else:
-            cl = a.cluster
+        cl = max(0, a.cluster)   # 0: fused form; > 0: one cluster of that size per model
         kw = {"batched": True, "cluster": cl}
     else:
         if a.concurrency <= 0:
@@ -195,7 +194,7 @@ def bench_serving(a):
     budget = min(150e9, torch.cuda.mem_get_info(dev)[0] * 0.85)
     clocks = ClockSampler(0)
     clocks.start()
-    reqs, st = Server(device=dev, slots=a.slots, hbm_budget=budget, batched=not a.unbatched,
+    reqs, st = Server(device=dev, slots=a.slots, hbm_budget=budget, batched=not a.streams,
                       cluster=a.cluster).replay(trace)
     clk = clocks.stop()
     print(json.dumps({
