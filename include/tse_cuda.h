@@ -331,6 +331,19 @@ int32_t tse_mass_totals(const TseGrid *grid, const double *phi,
                         const double *WP, const double *WT, double *d_out,
                         void *d_workspace, size_t workspace_bytes, void *stream);
 
+/* Self-test of the bounded waits (no counterpart in the reference).  Every
+ * persistent kernel here waits on other blocks (grid barriers) or on its own
+ * bulk copies (mbarriers), and each of those waits gives up after a time
+ * limit, raises an error flag and lets the kernel return with
+ * TSE_STATUS_BARRIER_TIMEOUT.  This call runs each kind of wait -- the
+ * generation grid barrier, the counter grid barrier, the mbarrier wait --
+ * against a condition that never comes true, with a limit of timeout_s
+ * seconds (at most 5), and writes to d_result[0..2] 1 for each wait that gave
+ * up and raised its flag, 0 otherwise.  d_ws: at least 512 bytes of device
+ * memory.  Takes about 3 * timeout_s; nothing faults or hangs. */
+int32_t tse_selftest_bounded_waits(int32_t *d_result, double timeout_s, void *d_ws,
+                                   size_t ws_bytes, void *stream);
+
 /* Library version string. */
 const char *tse_version(void);
 

@@ -100,3 +100,10 @@ def test_batch_entry_points_validate_without_gpu():
         assert fn(items, 0, ct.byref(opts), ws, 1 << 20, None) == -1
         # NaN dt would halve forever: refused
         assert fn(items, 1, ct.byref(opts), ws, 1 << 20, None) == -1
+
+
+def test_selftest_validates_without_gpu():
+    L = N.lib()
+    assert L.tse_selftest_bounded_waits(None, 0.1, None, 0, None) == -1
+    assert L.tse_selftest_bounded_waits(ct.c_void_p(16), 0.1, ct.c_void_p(4096), 100, None) == -1
+    assert L.tse_selftest_bounded_waits(ct.c_void_p(16), 0.0, ct.c_void_p(4096), 512, None) == -1

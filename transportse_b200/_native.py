@@ -123,6 +123,7 @@ SIGNATURES = {
     "tse_peclet_T": (_I, [_G, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _S, _P]),
     "tse_mass_totals": (_I, [_G, _P, _P, _P, _PP, _PP, _I, _P, _P, _P, _P, _P, _P, _P, _P, _S,
                              _P]),
+    "tse_selftest_bounded_waits": (_I, [_P, _D, _P, _S, _P]),
     "tse_version": (ct.c_char_p, []),
 }
 

@@ -32,6 +32,7 @@ SOURCES = {
     "tse_capi.cu": ["--fmad=false"],
     "tse_dc.cu": [],
     "tse_batch.cu": [],
+    "tse_selftest.cu": [],
 }
 
 

@@ -63,7 +63,8 @@ struct GridBarrier {
     int pad;
 };
 
-__device__ __forceinline__ bool grid_sync(GridBarrier* b, unsigned nblocks) {
+__device__ __forceinline__ bool grid_sync(GridBarrier* b, unsigned nblocks,
+                                          unsigned long long timeout_ns = kBarrierTimeoutNs) {
     __syncthreads();
     if (nblocks == 1) return true;
     __shared__ int s_ok;
@@ -81,7 +82,7 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* b, unsigned nblocks) {
             unsigned spins = 0;
             while (ld_acquire_u32(&b->gen) == g) {
                 if (*(volatile int*)&b->error) { ok = 0; break; }
-                if ((++spins & 255u) == 0u && globaltimer() - t0 > kBarrierTimeoutNs) {
+                if ((++spins & 255u) == 0u && globaltimer() - t0 > timeout_ns) {
                     atomicExch(&b->error, 1);
                     ok = 0;
                     break;

@@ -362,13 +362,14 @@ static_assert(kTmaChunk % kTmaGroup == 0, "whole cells per consumer thread");
 
 // wait for a phase of `bar`; gives up (false) when the block's error flag is
 // raised or after kBarrierTimeoutNs, raising the flag
-__device__ __forceinline__ bool mbar_wait_flag(uint64_t* bar, unsigned parity, volatile int* err) {
+__device__ __forceinline__ bool mbar_wait_flag(uint64_t* bar, unsigned parity, volatile int* err,
+                                               unsigned long long timeout_ns = kBarrierTimeoutNs) {
     if (mbar_try_wait(bar, parity)) return true;
     const uint64_t t0 = globaltimer();
     unsigned spins = 0;
     while (!mbar_try_wait(bar, parity)) {
         if (*err) return false;
-        if ((++spins & 63u) == 0u && globaltimer() - t0 > kBarrierTimeoutNs) {
+        if ((++spins & 63u) == 0u && globaltimer() - t0 > timeout_ns) {
             *err = 1;
             return false;
         }
@@ -388,7 +389,8 @@ __device__ __forceinline__ void red_release_add(unsigned* p, unsigned v) {
 // between the last arrival and the waiters' release.  Bounded like
 // grid_sync: on timeout (or another block's error) the error flag is raised
 // and false returned.
-__device__ __forceinline__ bool count_sync(unsigned* counter, unsigned target, GridBarrier* bar) {
+__device__ __forceinline__ bool count_sync(unsigned* counter, unsigned target, GridBarrier* bar,
+                                           unsigned long long timeout_ns = kBarrierTimeoutNs) {
     __syncthreads();
     __shared__ int s_ok;
     if (threadIdx.x == 0) {
@@ -399,7 +401,7 @@ __device__ __forceinline__ bool count_sync(unsigned* counter, unsigned target, G
             unsigned spins = 0;
             while (ld_acquire_u32(counter) < target) {
                 if (*(volatile int*)&bar->error) { ok = 0; break; }
-                if ((++spins & 255u) == 0u && globaltimer() - t0 > kBarrierTimeoutNs) {
+                if ((++spins & 255u) == 0u && globaltimer() - t0 > timeout_ns) {
                     atomicExch(&bar->error, 1);
                     ok = 0;
                     break;
