@@ -56,6 +56,8 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--shape", type=str, default=None, help="override grid, e.g. 64x64x32")
+    ap.add_argument("--dc-cycle", type=int, default=0,
+                    help="iterations per FP32 correction cycle (0: the model's default)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -528,6 +530,8 @@ def main():
 
     # ---- headline: FP32 sweeps + FP64 defect correction
     sim = Simulation(workloads.reservoir_3d(*shape), device=dev, precision="fp32dc")
+    if a.dc_cycle:
+        sim.M.dc_cycle = int(a.dc_cycle)
     for _ in range(a.warmup):
         sim.run(max_steps=1)
     res = timed_steps(ctx, sim, a.steps, ClockSampler(local))

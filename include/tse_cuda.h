@@ -139,7 +139,7 @@ int32_t tse_compute_P(const TseGrid *grid, const TsePressureArgs *args,
  * sweep kernel's event record) and return when the solve is done.
  * Workspace: TSE_WS_PRESSURE_DC / TSE_WS_TRANSPORT_DC. */
 typedef struct TseDcOptions {
-    int32_t cycle;            /* in: iterations per correction cycle, <= 0: 128 */
+    int32_t cycle;            /* in: iterations per correction cycle, <= 0: 256 */
     int32_t max_blocks;       /* in: cap on the sweep kernel's blocks, <= 0: as
                                  many as fit; lets several solves share the GPU */
     int32_t timing;           /* in: 1 = time the sweep-kernel launches with

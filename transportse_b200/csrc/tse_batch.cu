@@ -321,7 +321,7 @@ static void fill_ctl(DcCtl& c, double inc_it, double max_dt, double min_dt, doub
     c.max_it = max_it;
     c.pressure_schedule = pressure_schedule;
     c.stop_on_first = stop_on_first;
-    c.cycle = (opts && opts->cycle > 0) ? opts->cycle : 128;
+    c.cycle = (opts && opts->cycle > 0) ? opts->cycle : 256;
     c.sor = (float)sor;
 }
 

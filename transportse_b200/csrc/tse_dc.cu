@@ -698,7 +698,7 @@ static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, 
     c.max_it = max_it;
     c.pressure_schedule = pressure_schedule;
     c.stop_on_first = stop_on_first;
-    c.cycle = cycle > 0 ? cycle : 128;
+    c.cycle = cycle > 0 ? cycle : 256;
     c.sor = (float)sor;
     const long long dlen = dc_delta_len(S.L, S.Ncal);
     float* dbase = c.D[0] - dc_margin(S.L);

@@ -35,7 +35,7 @@ class Model:
     PRECISIONS = ("fp64", "fp32dc")
 
     def __init__(self, nx, ny, nz, dx, dy, dz, g, beta_deg, device=None, precision="fp64",
-                 dc_cycle=128):
+                 dc_cycle=256):
         """precision 'fp64': the reference's arithmetic, operation for
         operation; 'fp32dc': FP32 sweeps on a correction driven by an FP64
         residual (tse_compute_*_dc), same convergence test and dt control."""
@@ -88,7 +88,7 @@ class Model:
             precision = getattr(config, "GPU_PRECISION", "fp64")
         return cls(config.nx, config.ny, config.nz, config.dx, config.dy, config.dz, config.g,
                    config.beta, device=device, precision=precision,
-                   dc_cycle=getattr(config, "GPU_DC_CYCLE", 128))
+                   dc_cycle=getattr(config, "GPU_DC_CYCLE", 256))
 
     # FP32 corrections resolve a relative change of about 1e-13 of the FP64
     # iterate at best; a solve asking for a tighter tolerance runs in FP64
