@@ -75,12 +75,9 @@ def parse_args():
                     help="ensemble, unbatched: models in flight (0 = autotune)")
     ap.add_argument("--cluster", type=int, default=0,
                     help="ensemble/serving, batched: CTAs per model (0 = autotune / 8)")
-    ap.add_argument("--batched", action="store_true",
-                    help="ensemble: lock-step batched solves (one launch per solve kind) instead "
-                         "of concurrent per-model streams (the default)")
     ap.add_argument("--streams", action="store_true",
-                    help="serving: concurrent per-slot streams instead of batched solves "
-                         "(the default)")
+                    help="ensemble/serving: concurrent per-model streams instead of batched "
+                         "solves (one fused launch per solve kind, the default)")
     ap.add_argument("--requests", type=int, default=40, help="serving: requests")
     ap.add_argument("--rate", type=float, default=20.0, help="serving: arrivals per second")
     ap.add_argument("--slots", type=int, default=8, help="serving: concurrent models")
@@ -100,7 +97,7 @@ def bench_ensemble(a):
     nmax = a.n_max or 128
     cfgs = [workloads.ensemble_member(seed=1000 + i, n_max=nmax) for i in range(a.models)]
     tune = None
-    batched = a.batched
+    batched = not a.streams
     conc = cyc = cl = None
     if batched:
         cl = max(0, a.cluster)   # 0: fused form; > 0: one cluster of that size per model

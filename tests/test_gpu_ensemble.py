@@ -34,7 +34,7 @@ def test_ensemble_alone_equals_mixed(precision, mode, tol, cuda_device):
     steps = 3
     batched = mode == "batched"
     alone, _ = Ensemble(_configs(), device=cuda_device, precision=precision,
-                        concurrency=1, cluster_cells=0).run(steps)
+                        concurrency=1, batched=False, cluster_cells=0).run(steps)
     mixed, stats = Ensemble(_configs(), device=cuda_device, precision=precision,
                             concurrency=None if batched else 4, batched=batched,
                             cluster_cells=(1 << 30) if mode == "cluster" else 0).run(steps)

@@ -8,17 +8,16 @@ thread on its own CUDA stream through the full time-step driver
 model progresses at its own pace.  Models are admitted as earlier ones finish
 and their device memory is returned, under an HBM budget.
 
-How a model's mixed-precision solves run depends on its size:
+By default (``batched``, mixed-precision form) the models' threads meet at a
+``BatchGate`` (transportse_b200.batch): each kind of solve of all models runs
+as one fused launch -- every model's cells in one cooperative sweep sharing
+its barriers, finished models dropping out -- so small models cost their
+bytes rather than two device-wide barriers per iteration.  With
+``batched=False`` each model solves on its own stream:
   * grids of up to ``cluster_cells`` cells: each solve is one launch of one
-    thread-block cluster (tse_compute_*_dc_batch with one item) -- no
-    device-wide barrier, no host round trip -- so many small models stream
-    side by side;
+    thread-block cluster (tse_compute_*_dc_batch with one item);
   * larger grids: the cooperative whole-GPU sweeps, each capped to its share
     of the co-resident blocks.
-With ``batched=True`` the threads instead meet at a ``BatchGate``
-(transportse_b200.batch), which runs each kind of solve of all waiting models
-as one launch in lock step; that suits ensembles of equal models, since a
-batch lasts as long as its slowest member.
 
 More than eight concurrent streams need CUDA_DEVICE_MAX_CONNECTIONS raised
 (e.g. to 32) before the process creates its CUDA context, or their launches
@@ -202,17 +201,18 @@ CLUSTER_CELLS = 0
 
 class Ensemble:
     """``concurrency``: models in flight (None: 4, or every model when
-    batched).  ``batched``: solve in lock step through a BatchGate.
+    batched).  ``batched``: solve in lock step through a BatchGate (None: for
+    the mixed-precision form).
     ``cluster``: CTAs per model in cluster launches (0: 16 alone, 8 batched).
     ``cluster_cells``: largest grid (cells) solved by single-cluster launches
     when not batched (None: CLUSTER_CELLS)."""
 
     def __init__(self, configs, device=None, precision="fp32dc", concurrency=None, hbm_budget=None,
-                 max_blocks=None, dc_cycle=None, batched=False, cluster=0, cluster_cells=None):
+                 max_blocks=None, dc_cycle=None, batched=None, cluster=0, cluster_cells=None):
         self.configs = list(configs)
         self.device = torch.device(device if device is not None else "cuda")
         self.precision = precision
-        self.batched = bool(batched)
+        self.batched = (precision == "fp32dc") if batched is None else bool(batched)
         if self.batched and precision != "fp32dc":
             raise ValueError("batched solves need precision='fp32dc'")
         self.cluster_cells = CLUSTER_CELLS if cluster_cells is None else int(cluster_cells)
