@@ -48,8 +48,8 @@ constexpr int kSweepBlock = TSE_SWEEP_BLOCK;
 #ifndef TSE_TMA_ROUNDSYNC
 #define TSE_TMA_ROUNDSYNC 0  // 1: colour phases ordered per round of chunks, device-wide
                              // barrier only before a check's sums (measured 2.7x slower:
-                             // the per-chunk proxy fence and GPU-scope release sit on
-                             // the critical path)
+                             // the GPU-scope release/acquire per chunk sits on the
+                             // critical path)
 #endif
 #ifndef TSE_TMA_PREFETCH
 #define TSE_TMA_PREFETCH 1   // 1: a phase's own parts are copied before its grid barrier
