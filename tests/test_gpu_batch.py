@@ -67,6 +67,9 @@ def _pressure_case(shape, seed):
 
 
 SHAPES = [(33, 17, 21), (1, 1, 40), (16, 16, 16), (9, 1, 31), (40, 30, 24), (5, 7, 3)]
+# column heights far apart in one batch: the stage layout is sized for the
+# tallest column, each model's windows for its own
+MIXED_H = [(2, 2, 600), (60, 40, 2), (12, 9, 7)]
 
 
 @pytest.mark.parametrize("cluster", [0, 1, 4, 16])
@@ -153,3 +156,26 @@ def test_batched_unit_calls_match_reference_fixtures(cuda_device):
                     assert abs(t - ref[0]) <= 1e-12 * abs(ref[0]), name
             else:
                 assert rel_err(g, ref) <= TOL, (v, name, rel_err(g, ref))
+
+
+def test_fused_batch_with_far_apart_column_heights(cuda_device):
+    kw = dict(SOR=1.7, max_it=20000, inc_it=1.25, max_dt=1e5, min_dt=1e-8, P_conv=1e-10)
+    cases_ = [_pressure_case(s, 90 + i) for i, s in enumerate(MIXED_H)]
+
+    def member(i):
+        cfg, P, rest = cases_[i]
+
+        def fn(gate):
+            m = model_for(cfg, cuda_device, "fp32dc")
+            m.batch_gate = gate
+            return NumpyKernels(m).compute_P(P.copy(), *rest, **kw)
+        return fn
+
+    got, gate = _run_members([member(i) for i in range(len(MIXED_H))], cuda_device, 0)
+    assert gate.stats()["launches"]["compute_P"] == 1
+    for i, g in enumerate(got):
+        cfg, P, rest = cases_[i]
+        ro = OracleModel(cfg).compute_P(P.copy(), *rest, **kw)
+        assert g[4] == ro[4] and g[0] == ro[0] and g[1] == ro[1], MIXED_H[i]
+        assert abs(g[5] - ro[5]) <= max(10, 0.05 * ro[5]), (MIXED_H[i], g[5], ro[5])
+        assert rel_err(g[2], ro[2]) <= TOL, MIXED_H[i]
