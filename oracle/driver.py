@@ -40,6 +40,40 @@ SNAPSHOT_ITEMS = ("lx", "ly", "lz", "nx", "ny", "nz", "dx", "dy", "dz", "t_sim",
                   "nue", "cp_f", "l_f", "BP", "BC", "BT", "L", "mass", "WP", "WT", "WC", "e")
 
 
+def chemistry(config, S, t_sim, dt, chem):
+    """The chemistry coupling of tse.py:1383-1417, once per Picard iteration:
+    chem_inc accumulates dt (after the first step), and once it reaches
+    DTCHEM (or in the first step) the config's chemical_reactions_all runs on
+    the whole state, or chemical_reactions on each cell whose BC is not 1
+    (k, j, i order, joblib with parallel_chemistry jobs)."""
+    if t_sim > 0:
+        chem["inc"] += dt
+    else:
+        chem["inc"] = 0
+        chem["dt_chem"] = dt
+    if chem["inc"] >= config.DTCHEM:
+        chem["dt_chem"] = chem["inc"]
+        chem["inc"] = 0
+    BC = S["BC"]
+    nx, ny, nz = BC.shape[:3]
+    cells = [(i, j, k) for k in range(nz) for j in range(ny) for i in range(nx) if BC[i, j, k] != 1]
+    if cells == [] or chem["inc"] != 0:
+        return
+    names = ("C", "P", "T", "rho_f", "phi", "Kx", "Ky", "Kz")
+    if hasattr(config, "chemical_reactions_all"):
+        out = config.chemical_reactions_all(*[S[n] for n in names], chem["dt_chem"])
+        for n, v in zip(names, out):
+            S[n] = v
+    else:
+        from joblib import Parallel, delayed
+        res = Parallel(n_jobs=config.parallel_chemistry)(
+            delayed(config.chemical_reactions)(*[S[n][i, j, k] for n in names], chem["dt_chem"],
+                                               i, j, k) for i, j, k in cells)
+        for (i, j, k), r in zip(cells, res):
+            for n, v in zip(names, r):
+                S[n][i, j, k] = v
+
+
 class Plots:
     """plotresults (tse.py:312-329): with PLOTSAVE, shorten dt so the run
     lands on the next PLOTTIME (remembering the unshortened dt in dt_prev);
@@ -103,8 +137,6 @@ def run(config, max_steps=None, on_step=None, verbose=False, plot_prefix=None):
     """Run the config; returns the final state dict (plus 'n_tsteps', 't_sim',
     'plots' = snapshot files written).  Snapshots go to
     "<plot_prefix>-<k:05d>.p" (default: the config module's name)."""
-    if config.CHEMREACT:
-        raise NotImplementedError("chemistry coupling is outside the time-step core")
     S = {}
     for name in FIELDS:
         S[name] = numpy.array(getattr(config, name), dtype=numpy.float64, copy=True)
@@ -150,6 +182,7 @@ def run(config, max_steps=None, on_step=None, verbose=False, plot_prefix=None):
         return tuple(v[k] if k in v else S[k] for k in SNAPSHOT_ITEMS)
 
     dt_prev = dt                     # tse.py:1121
+    chem = {"inc": 0, "dt_chem": 0}  # tse.py:1132-1133
     dt, dt_prev = plots(t_sim, dt, dt_prev, snapshot)   # tse.py:1177
     while t_sim < t:
         SIA_filled = False
@@ -260,6 +293,8 @@ def run(config, max_steps=None, on_step=None, verbose=False, plot_prefix=None):
                     num_it_T += num_itT
                     if not conv:
                         raise ConvergenceError("* T CONVERGENCE ERROR - check dt and T_conv in compute_T")
+            if config.CHEMREACT:
+                chemistry(config, S, t_sim, dt, chem)
             if config.FLUIDPROP:
                 update_fluid_properties(config, S)
             if config.SIA:

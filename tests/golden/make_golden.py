@@ -171,6 +171,9 @@ E2E = {
     "serving_request": (workloads.serving_request, {"seed": 4, "n": 9},
                         5, {1, 5}, ("P", "C", "T", "qz")),
     "slice_2d_plot": (workloads.slice_2d_plot, {}, 100, {1, 50, 100}, ("P", "C", "qx", "qz")),
+    "slice_2d_chem": (workloads.slice_2d_chem, {}, 24, {1, 2, 3, 12, 24}, ("P", "C", "phi", "qz")),
+    "slice_2d_chemcell": (workloads.slice_2d_chem, {"per_cell": True}, 8, {1, 2, 3, 8},
+                          ("P", "C", "phi", "qz")),
 }
 
 

@@ -95,9 +95,6 @@ class Simulation:
         sweeps with FP64 defect correction); default: config.GPU_PRECISION,
         else 'fp64'.  plot_prefix: path prefix of the PLOTSAVE snapshot files
         (default: the config module's name, in the working directory)."""
-        if config.CHEMREACT:
-            raise NotImplementedError("CHEMREACT: chemistry coupling is not part of the GPU "
-                                      "time-step core")
         if getattr(config, "NLTE_SOLV", False) and config.SMOLAR_T:
             raise NotImplementedError("NLTE_SOLV with SMOLAR_T is not supported by the reference")
         self.config = config
@@ -326,6 +323,8 @@ class Simulation:
                         num_it_T += num_itT
                         if not conv:
                             raise ConvergenceError("* T CONVERGENCE ERROR - check dt and T_conv in compute_T")
+                if cfg.CHEMREACT:
+                    self._chemistry(dt)
                 if cfg.FLUIDPROP:
                     self.update_fluid_properties()
                 if cfg.SIA:
@@ -405,6 +404,49 @@ class Simulation:
         self._bc_inc = new_inc
         if new_inc != bc_inc and cfg.FLUIDPROP:
             self.update_fluid_properties()
+
+    def _chemistry(self, dt):
+        """Chemistry coupling (tse.py:1383-1417), a host hook once per Picard
+        iteration: chem_inc accumulates dt (after the first step); when it
+        reaches DTCHEM (and in the first step) the state goes to the host, the
+        config's chemical_reactions_all runs on it -- or chemical_reactions on
+        each cell whose BC is not 1, k-j-i order, through joblib with
+        parallel_chemistry jobs -- and the results come back to the device."""
+        cfg = self.config
+        st = self.__dict__.setdefault("_chem", {"inc": 0, "dt_chem": 0})
+        if self.t_sim > 0:
+            st["inc"] += dt
+        else:
+            st["inc"] = 0
+            st["dt_chem"] = dt
+        if st["inc"] >= cfg.DTCHEM:
+            st["dt_chem"] = st["inc"]
+            st["inc"] = 0
+        if st["inc"] != 0:
+            return
+        BC = self.field("BC")
+        kk, jj, ii = numpy.nonzero(numpy.transpose(BC != 1, (2, 1, 0)))   # k, j, i order
+        if len(ii) == 0:
+            return
+        names = ("C", "P", "T", "rho_f", "phi", "Kx", "Ky", "Kz")
+        h = {n: self.field(n) for n in names}
+        if hasattr(cfg, "chemical_reactions_all"):
+            out = cfg.chemical_reactions_all(*[h[n] for n in names], st["dt_chem"])
+            h = dict(zip(names, out))
+        else:
+            from joblib import Parallel, delayed
+            cells = list(zip(ii.tolist(), jj.tolist(), kk.tolist()))
+            res = Parallel(n_jobs=cfg.parallel_chemistry)(
+                delayed(cfg.chemical_reactions)(*[h[n][i, j, k] for n in names], st["dt_chem"],
+                                                i, j, k) for i, j, k in cells)
+            for (i, j, k), r in zip(cells, res):
+                for n, v in zip(names, r):
+                    h[n][i, j, k] = v
+        for n in names:
+            a = numpy.asarray(h[n], dtype=numpy.float64)
+            if n in FIELDS4 or (n == "T" and a.ndim == 4):
+                a = numpy.moveaxis(a, 3, 0)
+            self.S[n].copy_(torch.as_tensor(numpy.ascontiguousarray(a)))
 
     def _mass_balance(self, dt):
         """Mass balance at the point of tse.py:1460-1463: FP64 device totals

@@ -220,6 +220,39 @@ def slice_2d_plot(nx=60, ny=1, nz=30, steps=100, t_last=2.0e7, n_plot=6):
     return m
 
 
+CHEM_RATE = 2e-7   # 1/s, first-order decay of the slice_2d_chem species
+
+
+def chem_decay_all(C, P, T, rho_f, phi, Kx, Ky, Kz, dt_chem):
+    """Vectorised chemistry of slice_2d_chem (the chemical_reactions_all hook):
+    first-order decay of every species, porosity growing with what decayed."""
+    f = math.exp(-CHEM_RATE * dt_chem)
+    return C * f, P, T, rho_f, phi * (1.0 + 1e-3 * (1.0 - f)), Kx, Ky, Kz
+
+
+def chem_decay_cell(c, p, t, rho_f, phi, kx, ky, kz, dt_chem, i, j, k):
+    """The same chemistry one cell at a time (the chemical_reactions hook)."""
+    f = math.exp(-CHEM_RATE * dt_chem)
+    return c * f, p, t, rho_f, phi * (1.0 + 1e-3 * (1.0 - f)), kx, ky, kz
+
+
+def slice_2d_chem(nx=60, ny=1, nz=30, steps=40, per_cell=False):
+    """slice_2d with chemistry coupling on (tse.py:1383-1417): every DTCHEM of
+    accumulated step time the chemistry runs on every cell whose species
+    boundary flag is not 1, through chemical_reactions_all (vectorised) or,
+    with per_cell, chemical_reactions one cell at a time."""
+    m = slice_2d(nx, ny, nz, steps)
+    m.__name__ = "slice_2d_chemcell" if per_cell else "slice_2d_chem"
+    m.CHEMREACT = True
+    m.DTCHEM = 2 * 86400.0
+    m.parallel_chemistry = 1
+    if per_cell:
+        m.chemical_reactions = chem_decay_cell
+    else:
+        m.chemical_reactions_all = chem_decay_all
+    return m
+
+
 def reservoir_3d(nx=256, ny=256, nz=128, seed=2024, steps=100):
     """Bottom-heated 3-D reservoir with a dense brine patch on top.
 
