@@ -185,6 +185,25 @@ def gen_e2e(ref, name):
     return data
 
 
+LOGS = {
+    # name: (builder, kwargs, steps) -- the reference's per-step log lines
+    "slice_2d": (workloads.slice_2d, {}, 30),
+    "reservoir_3d": (workloads.reservoir_3d, {"nx": 12, "ny": 10, "nz": 8, "seed": 11}, 6),
+}
+
+
+def gen_log(ref, name):
+    """The lines tse.py prints for every step (PRINTOUT = 1), from the first
+    flow line on; the run stops inside the last step, after its flow lines."""
+    builder, kw, steps = LOGS[name]
+    cfg = builder(**kw)
+    cfg.PRINTOUT = 1
+    _, ns = run_reference(ref, cfg, steps, set(), ())
+    lines = ns["__stdout__"].split("\n")
+    first = [k for k, l in enumerate(lines) if "[CFL]" in l][0]
+    return "\n".join(lines[first:]).rstrip("\n") + "\n"
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default=os.environ.get("TSE_REFERENCE", "/root/reference"))
@@ -193,6 +212,13 @@ def main():
     jobs = [("unit_a", lambda: gen_unit(a.reference, "a")),
             ("unit_b", lambda: gen_unit(a.reference, "b"))]
     jobs += [("e2e_" + n, (lambda n=n: gen_e2e(a.reference, n))) for n in E2E]
+    for name in LOGS:
+        if a.only and a.only != "log_" + name:
+            continue
+        path = os.path.join(HERE, "log_%s.txt" % name)
+        with open(path, "w") as f:
+            f.write(gen_log(a.reference, name))
+        print("wrote", path)
     for name, fn in jobs:
         if a.only and a.only != name:
             continue

@@ -365,8 +365,10 @@ class Simulation:
             self.n_tsteps += 1
             steps_here += 1
             if self.verbose and self.n_tsteps % cfg.PRINTOUT == 0:
-                print("[t] %8.2e/%8.2e [dt] %8.2e [S] %4d [P] %3d [C] %3d [T] %3d [CFL] %d"
-                      % (self.t_sim, t, dt, self.n_tsteps, num_it_P, num_it_C, num_it_T, CFL))
+                # tse.py:1481-1484, bold dt included
+                print("[t] %8.2e/%8.2e [dt] \033[1m%8.2e\033[0m [S] %4d [P] %3d"
+                      % (self.t_sim, t, dt, self.n_tsteps, num_it_P)
+                      + " [C] %3d [T] %3d [CFL] %d" % (num_it_C, num_it_T, CFL))
             dt = 1e99
             if cfg.FLUIDFLOW:
                 dt = pymin(dt_P, t - self.t_sim)
