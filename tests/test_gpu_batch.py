@@ -179,3 +179,22 @@ def test_fused_batch_with_far_apart_column_heights(cuda_device):
         assert g[4] == ro[4] and g[0] == ro[0] and g[1] == ro[1], MIXED_H[i]
         assert abs(g[5] - ro[5]) <= max(10, 0.05 * ro[5]), (MIXED_H[i], g[5], ro[5])
         assert rel_err(g[2], ro[2]) <= TOL, MIXED_H[i]
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32dc"])
+@pytest.mark.parametrize("case", ["nan_input", "max_it_1"])
+def test_failure_paths_follow_the_reference(precision, case, cuda_device):
+    """Non-convergence as the reference handles it: a NaN in the pressure (the
+    L2 change is NaN and counts as 1) or max_it = 1 makes every attempt fail,
+    dt is halved until it drops below min_dt, and the solve returns
+    unconverged -- same t, dt and iteration count as the oracle, no hang."""
+    cfg, P, rest = _pressure_case((9, 1, 31), 123)
+    if case == "nan_input":
+        P[4, 0, 10] = float("nan")
+        kw = dict(SOR=1.7, max_it=30, inc_it=1.25, max_dt=1e5, min_dt=400.0, P_conv=1e-10)
+    else:
+        kw = dict(SOR=1.7, max_it=1, inc_it=1.25, max_dt=1e5, min_dt=1.0, P_conv=1e-10)
+    ro = OracleModel(cfg).compute_P(P.copy(), *rest, **kw)
+    g = NumpyKernels(model_for(cfg, cuda_device, precision)).compute_P(P.copy(), *rest, **kw)
+    assert not ro[4] and not g[4]
+    assert g[0] == ro[0] and g[1] == ro[1] and g[5] == ro[5], (g[:2], g[5], ro[:2], ro[5])

@@ -180,3 +180,76 @@ def test_snapshot_rule_matches_the_oracle(tmp_path):
                 dt, dt_prev = step(t_sim, dt, dt_prev, lambda d, t=t_sim: (t, d))
             outs.append((seq, [p[-8:] for p in pl.written], pl.index))
         assert outs[0] == outs[1], times
+
+
+def _staged_copies_ok(nx, ny, nz, Hstage, C=512):
+    """Every bulk copy of the staged sweep for one model (the arithmetic of
+    tse_dc.cuh tma_stage / tma_issue_own / tma_issue_windows and of the
+    consumers' window indices) is 16-byte aligned, a multiple of 16 bytes,
+    inside its array, and every shared-memory index stays inside its window."""
+    nzp = nz + (nz & 1)
+    H = nzp // 2
+    SX = ny * H
+    Nc = nx * SX
+    N = (Nc + 31) & ~31
+    G = ((SX + 1024 + 16 + 63) // 64) * 64            # dc_margin
+    lz = lambda h: (C + 2 * h + 5 + 3) & ~3
+    lx = C + 4
+    assert lz(H) <= lz(Hstage)
+    base = 256 * 7                                      # any 256-aligned float region
+    K = [base, base + 28 * N]
+    dbase = base + 56 * N
+    dlen = N + 2 * G
+    D = [dbase + 4 * G, dbase + 4 * (dlen + G)]
+    Dlo = [dbase, dbase + 4 * dlen]
+    Dhi = [dbase + 4 * dlen, dbase + 8 * dlen]
+    mask = [0, ((N + 255) // 256) * 256]
+    for col in (0, 1):
+        for q in range((Nc + C - 1) // C):
+            m0 = q * C
+            cnt = min(C, N - m0)
+            zs, xps, xms = (m0 - H - 1) & ~3, (m0 + SX) & ~3, (m0 - SX) & ~3
+            copies = [(K[col] + 24 * m0, 24 * cnt, K[col], K[col] + 24 * N),
+                      (K[col] + 24 * N + 4 * m0, 4 * cnt, K[col] + 24 * N, K[col] + 28 * N),
+                      (mask[col] + m0, cnt, mask[col], mask[col] + N),
+                      (D[col] + 4 * m0, 4 * cnt, Dlo[col], Dhi[col]),
+                      (D[1 - col] + 4 * zs, 4 * lz(H), Dlo[1 - col], Dhi[1 - col]),
+                      (D[1 - col] + 4 * xps, 4 * lx, Dlo[1 - col], Dhi[1 - col]),
+                      (D[1 - col] + 4 * xms, 4 * lx, Dlo[1 - col], Dhi[1 - col])]
+            for a, n, lo, hi in copies:
+                if a % 16 or n % 16 or a < lo or a + n > hi:
+                    return False
+            oz, oxp, oxm = m0 - zs, m0 + SX - xps, m0 - SX - xms
+            nval = min(C, Nc - m0)
+            l = nval - 1
+            if not (0 <= oz - H - 1 and l + oz + H < lz(H) and 0 <= oxp and l + oxp < lx
+                    and 0 <= oxm and l + oxm < lx):
+                return False
+    return True
+
+
+def test_staged_sweep_copies_stay_aligned_and_in_bounds():
+    import random
+    rng = random.Random(5)
+    shapes = [(1, 1, 1), (1, 1, 2), (2, 1, 1), (3, 3, 3), (1, 1, 40), (9, 1, 31), (5, 7, 3),
+              (60, 1, 30), (33, 17, 21), (2, 2, 600), (60, 40, 2), (64, 64, 32), (128, 96, 77)]
+    shapes += [(rng.randint(1, 40), rng.randint(1, 40), rng.randint(1, 300)) for _ in range(60)]
+    # single model: the stage fits its own H; fused batch: the tallest column's
+    Hmax = max((nz + (nz & 1)) // 2 for _, _, nz in shapes)
+    for nx, ny, nz in shapes:
+        H = (nz + (nz & 1)) // 2
+        assert _staged_copies_ok(nx, ny, nz, H), (nx, ny, nz)
+        assert _staged_copies_ok(nx, ny, nz, Hmax), (nx, ny, nz, "fused")
+
+
+def test_server_cancels_pending_requests():
+    """A request that has not started can be withdrawn; the others stay queued."""
+    from transportse_b200 import workloads
+    from transportse_b200.serving import Request, Server
+    s = Server(device="cpu", slots=1, hbm_budget=1 << 40, max_blocks=8)
+    a = s.submit(Request(0, workloads.serving_request(1, n=8), 1, 0.0))
+    b = s.submit(Request(1, workloads.serving_request(2, n=8), 1, 0.1))
+    assert s.cancel(0) is True
+    assert a.cancelled and a.done.is_set() and a.error is not None
+    assert s.cancel(0) is False and s.cancel(7) is False
+    assert [item[1] for item in s.pending] == [1] and not b.done.is_set()

@@ -40,6 +40,7 @@ class Request:
         self.finish = None
         self.result = None
         self.error = None
+        self.cancelled = False
         self.done = threading.Event()
 
     @property
@@ -86,6 +87,22 @@ class Server:
             heapq.heappush(self.pending, (req.arrival, req.rid, req))
             self.cv.notify()
         return req
+
+    def cancel(self, rid):
+        """Withdraw a request that has not started; True if it was pending.
+        A request already on the GPU runs to its end."""
+        with self.cv:
+            for k, item in enumerate(self.pending):
+                if item[1] == rid:
+                    req = item[2]
+                    self.pending[k] = self.pending[-1]
+                    self.pending.pop()
+                    heapq.heapify(self.pending)
+                    req.error = RuntimeError("request %s cancelled" % rid)
+                    req.cancelled = True
+                    req.done.set()
+                    return True
+        return False
 
     def _next(self):
         with self.cv:
