@@ -198,3 +198,41 @@ def test_failure_paths_follow_the_reference(precision, case, cuda_device):
     g = NumpyKernels(model_for(cfg, cuda_device, precision)).compute_P(P.copy(), *rest, **kw)
     assert not ro[4] and not g[4]
     assert g[0] == ro[0] and g[1] == ro[1] and g[5] == ro[5], (g[:2], g[5], ro[:2], ro[5])
+
+
+def test_batched_driver_runs_match_reference_runs(cuda_device, tmp_path):
+    """Every reference end-to-end run at once, each model on its own thread
+    with its own number of steps, all mixed-precision solves batched through
+    one gate (models leave the batch as they finish): each matches its
+    reference run within 1e-6, dt sequence included."""
+    from tests.golden.make_golden import E2E
+    from transportse_b200.driver import Simulation
+    names = sorted(E2E)
+
+    def member(name):
+        def fn(gate):
+            builder, kw, steps, keep, fields = E2E[name]
+            sim = Simulation(builder(**kw), device=cuda_device, precision="fp32dc",
+                             plot_prefix=str(tmp_path / name))
+            sim.M.batch_gate = gate
+            got, dts = {}, []
+
+            def tap(rec, s):
+                dts.append(rec["dt"])
+                if rec["step"] in keep:
+                    for f in fields:
+                        got["%s@%d" % (f, rec["step"])] = s.field(f)
+            sim.run(max_steps=steps, on_step=tap)
+            return got, dts
+        return fn
+
+    out, gate = _run_members([member(n) for n in names], cuda_device)
+    st = gate.stats()
+    assert sum(st["solves"].values()) > sum(st["launches"].values())
+    for name, (got, dts) in zip(names, out):
+        fx = load("e2e_" + name)
+        # CFL-limited steps take dt from the fluxes, which carry the form's error
+        assert rel_err(numpy.array(dts), fx["s_dt"]) <= TOL, name
+        for k in fx.files:
+            if "@" in k and k.split("@")[0] in ("P", "C", "T"):
+                assert rel_err(got[k], fx[k]) <= TOL, (name, k, rel_err(got[k], fx[k]))
