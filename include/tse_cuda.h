@@ -167,7 +167,9 @@ int32_t tse_compute_T_dc(const TseGrid *grid, const TseHeatArgs *args,
  * tse_compute_*_dc -- its own grid, arguments, status record and workspace
  * (TSE_WS_PRESSURE_DC / TSE_WS_TRANSPORT_DC; no two items may share one) --
  * and gets the same results to the solver tolerance.  opts->cycle as for the
- * single-model form; the timing fields are not written.
+ * single-model form.  With opts->timing, the fused form writes the number of
+ * its sweep launches, the global iterations they ran and their summed CUDA
+ * event time (the cluster form writes nothing).
  *   opts->max_blocks <= 0: fused form -- every model's cells in one
  *     cooperative sweep sharing its barriers (models that finish drop out);
  *     the call synchronises the stream once per launch and returns when
@@ -201,13 +203,13 @@ typedef struct TseBatchHeat {
 } TseBatchHeat;
 size_t tse_batch_workspace_bytes(int32_t n, int64_t total_cells);
 int32_t tse_compute_P_dc_batch(const TseBatchPressure *items, int32_t n,
-                               const TseDcOptions *opts, void *d_batch_ws,
+                               TseDcOptions *opts, void *d_batch_ws,
                                size_t batch_ws_bytes, void *stream);
 int32_t tse_compute_C_dc_batch(const TseBatchSpecies *items, int32_t n,
-                               const TseDcOptions *opts, void *d_batch_ws,
+                               TseDcOptions *opts, void *d_batch_ws,
                                size_t batch_ws_bytes, void *stream);
 int32_t tse_compute_T_dc_batch(const TseBatchHeat *items, int32_t n,
-                               const TseDcOptions *opts, void *d_batch_ws,
+                               TseDcOptions *opts, void *d_batch_ws,
                                size_t batch_ws_bytes, void *stream);
 
 /* Pressure solve that allocates nothing and takes no workspace.  It has no

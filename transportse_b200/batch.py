@@ -66,6 +66,8 @@ class BatchGate:
         # statistics: launches per kind and models per launch
         self.launches = {k: 0 for k in KINDS}
         self.solves = {k: 0 for k in KINDS}
+        # fused form: sweep launches, global iterations, event ms per kind
+        self.sweeps = {k: [0, 0, 0.0] for k in KINDS}
 
     # ------------------------------------------------------- membership
     def join(self):
@@ -155,15 +157,20 @@ class BatchGate:
                                                 ct.c_void_p(r.status.data_ptr()),
                                                 ct.c_void_p(r.ws.data_ptr()), r.ws_bytes)
                                            for r in rs])
-                opts = N.TseDcOptions(cycle, self.cluster, 0)
+                opts = N.TseDcOptions(cycle, self.cluster, 1)
                 rc = getattr(L, "tse_%s_dc_batch" % name)(items, len(rs), ct.byref(opts),
                                                           ct.c_void_p(ws.data_ptr()), ws.numel(),
                                                           ct.c_void_p(bs.cuda_stream))
                 N.check(rc, "tse_%s_dc_batch" % name)
                 self.launches[name] += 1
                 self.solves[name] += len(rs)
+                self.sweeps[name][0] += opts.sweep_launches
+                self.sweeps[name][1] += opts.sweep_iterations
+                self.sweeps[name][2] += opts.sweep_ms
                 for r in rs:
                     r.stream.wait_stream(bs)
 
     def stats(self):
-        return {"launches": dict(self.launches), "solves": dict(self.solves)}
+        return {"launches": dict(self.launches), "solves": dict(self.solves),
+                "sweeps": {k: {"launches": v[0], "iterations": v[1], "ms": round(v[2], 3)}
+                           for k, v in self.sweeps.items()}}

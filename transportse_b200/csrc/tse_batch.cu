@@ -600,7 +600,8 @@ static size_t fused_ws_bytes(int n, long long cells) {
 }
 
 template <class Form>
-static int run_fused(std::vector<BatchItem<Form>>& v, void* d_ws, size_t ws_bytes, cudaStream_t stream) {
+static int run_fused(std::vector<BatchItem<Form>>& v, TseDcOptions* opts, void* d_ws, size_t ws_bytes,
+                     cudaStream_t stream) {
     const int n = (int)v.size();
     long long cells = 0;
     int Hmax = 0;
@@ -652,6 +653,16 @@ static int run_fused(std::vector<BatchItem<Form>>& v, void* d_ws, size_t ws_byte
     }
     int num_it = 0;
     int rc = TSE_OK;
+    // optional: launches, global iterations and event time of the fused sweeps
+    const bool timing = opts && opts->timing;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    if (timing) {
+        opts->sweep_launches = 0;
+        opts->sweep_iterations = 0;
+        opts->sweep_ms = 0.0;
+        if (cudaEventCreate(&ev0) != cudaSuccess || cudaEventCreate(&ev1) != cudaSuccess)
+            return TSE_ERR_LAUNCH;
+    }
     std::vector<FusedItem> hitems;
     std::vector<FusedChunk> hchunks;
     std::vector<DcState> got;
@@ -708,11 +719,13 @@ static int run_fused(std::vector<BatchItem<Form>>& v, void* d_ws, size_t ws_byte
             break;
         }
         void* args[] = {(void*)&A, (void*)&T};
+        if (timing) cudaEventRecord(ev0, stream);
         if (cudaLaunchCooperativeKernel((const void*)fused_sweep_kernel, dim3((unsigned)nb),
                                         dim3(kTmaThreads), args, smem, stream) != cudaSuccess) {
             rc = TSE_ERR_LAUNCH;
             break;
         }
+        if (timing) cudaEventRecord(ev1, stream);
         fused_gather_kernel<<<(na + 127) / 128, 128, 0, stream>>>(d_items, na, d_states);
         got.resize(na);
         if (cudaGetLastError() != cudaSuccess ||
@@ -724,6 +737,13 @@ static int run_fused(std::vector<BatchItem<Form>>& v, void* d_ws, size_t ws_byte
         }
         const int ran = got[0].num_it - num_it;
         num_it = got[0].num_it;
+        if (timing) {
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, ev0, ev1);
+            opts->sweep_launches += 1;
+            opts->sweep_iterations += ran;
+            opts->sweep_ms += ms;
+        }
         std::vector<int> next;
         bool failed = false;
         for (int k = 0; k < na; ++k) {
@@ -761,6 +781,10 @@ static int run_fused(std::vector<BatchItem<Form>>& v, void* d_ws, size_t ws_byte
         }
         active.swap(next);
     }
+    if (timing) {
+        cudaEventDestroy(ev0);
+        cudaEventDestroy(ev1);
+    }
     // status records and results of every model (a failed launch leaves
     // the models' state records as they were)
     for (auto& it : v) {
@@ -784,7 +808,7 @@ extern "C" size_t tse_batch_workspace_bytes(int32_t n, int64_t total_cells) {
 }
 
 extern "C" int32_t tse_compute_P_dc_batch(const TseBatchPressure* items, int32_t n,
-                                          const TseDcOptions* opts, void* d_batch_ws,
+                                          TseDcOptions* opts, void* d_batch_ws,
                                           size_t batch_ws_bytes, void* stream_) {
     if (!items || n < 1 || !d_batch_ws) return TSE_ERR_ARG;
     cudaStream_t stream = (cudaStream_t)stream_;
@@ -808,11 +832,11 @@ extern "C" int32_t tse_compute_P_dc_batch(const TseBatchPressure* items, int32_t
         v[i].cells = 2 * S.L.Nc;
     }
     if (opts && opts->max_blocks > 0) return launch_batch(v, opts, d_batch_ws, batch_ws_bytes, stream);
-    return run_fused(v, d_batch_ws, batch_ws_bytes, stream);
+    return run_fused(v, opts, d_batch_ws, batch_ws_bytes, stream);
 }
 
 extern "C" int32_t tse_compute_C_dc_batch(const TseBatchSpecies* items, int32_t n,
-                                          const TseDcOptions* opts, void* d_batch_ws,
+                                          TseDcOptions* opts, void* d_batch_ws,
                                           size_t batch_ws_bytes, void* stream_) {
     if (!items || n < 1 || !d_batch_ws) return TSE_ERR_ARG;
     cudaStream_t stream = (cudaStream_t)stream_;
@@ -837,11 +861,11 @@ extern "C" int32_t tse_compute_C_dc_batch(const TseBatchSpecies* items, int32_t 
         v[i].cells = 2 * S.L.Nc;
     }
     if (opts && opts->max_blocks > 0) return launch_batch(v, opts, d_batch_ws, batch_ws_bytes, stream);
-    return run_fused(v, d_batch_ws, batch_ws_bytes, stream);
+    return run_fused(v, opts, d_batch_ws, batch_ws_bytes, stream);
 }
 
 extern "C" int32_t tse_compute_T_dc_batch(const TseBatchHeat* items, int32_t n,
-                                          const TseDcOptions* opts, void* d_batch_ws,
+                                          TseDcOptions* opts, void* d_batch_ws,
                                           size_t batch_ws_bytes, void* stream_) {
     if (!items || n < 1 || !d_batch_ws) return TSE_ERR_ARG;
     cudaStream_t stream = (cudaStream_t)stream_;
@@ -866,5 +890,5 @@ extern "C" int32_t tse_compute_T_dc_batch(const TseBatchHeat* items, int32_t n,
         v[i].cells = 2 * S.L.Nc;
     }
     if (opts && opts->max_blocks > 0) return launch_batch(v, opts, d_batch_ws, batch_ws_bytes, stream);
-    return run_fused(v, d_batch_ws, batch_ws_bytes, stream);
+    return run_fused(v, opts, d_batch_ws, batch_ws_bytes, stream);
 }
