@@ -72,7 +72,8 @@ def parse_args():
     ap.add_argument("--models", type=int, default=48, help="ensemble: models")
     ap.add_argument("--n-max", type=int, default=None, help="ensemble/serving: largest axis")
     ap.add_argument("--concurrency", type=int, default=0,
-                    help="ensemble, unbatched: models in flight (0 = autotune)")
+                    help="ensemble: models in flight with --streams (0 = autotune); batched, "
+                         "any value > 0 skips the cycle-length autotune")
     ap.add_argument("--cluster", type=int, default=0,
                     help="ensemble/serving, batched: CTAs per model (0 = autotune / 8)")
     ap.add_argument("--streams", action="store_true",
@@ -101,6 +102,11 @@ def bench_ensemble(a):
     conc = cyc = cl = None
     if batched:
         cl = max(0, a.cluster)   # 0: fused form; > 0: one cluster of that size per model
+        if a.concurrency <= 0:
+            # the batched form's runtime knob: the correction-cycle length
+            tune = autotune(cfgs[:16], device=dev, steps=1, batched=True, clusters=(cl,),
+                            cycles=(128, 256, 512))
+            cyc = tune["dc_cycle"]
         kw = {"batched": True, "cluster": cl}
     else:
         if a.concurrency <= 0:
