@@ -97,82 +97,6 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* b, unsigned nblocks,
     return s_ok != 0;
 }
 
-// ------------------------------------------------------- neighbour sync
-// Phase synchronisation for the persistent solvers.  Each block owns one
-// contiguous chunk of the compact index range; a phase reads other blocks'
-// cells only within +-(SX + 1) indices, i.e. in the R nearest chunks on each
-// side.  After a phase a block publishes its phase number; before the next
-// phase it waits until its R neighbours on either side have published the
-// same number.  That orders every read after the neighbours' writes of the
-// previous phase and every write after their reads of it, without a
-// device-wide barrier.  `global()` is the full barrier, used where a
-// device-wide reduction follows.  Every wait is bounded in time.
-struct PhaseSync {
-    GridBarrier* bar;
-    unsigned* prog;   // one counter per block, zeroed before the launch
-    unsigned nb;
-    int R;            // neighbour radius in blocks (R >= nb: global only)
-    unsigned phase;
-
-    __device__ __forceinline__ void publish() {
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            __threadfence();
-            asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(prog + blockIdx.x), "r"(phase)
-                         : "memory");
-        }
-    }
-
-    __device__ __forceinline__ bool local() {
-        phase += 1;
-        if (nb == 1) { __syncthreads(); return true; }
-        if (R >= (int)nb) return global_keep_phase();
-        publish();
-        __shared__ int s_ok;
-        if (threadIdx.x == 0) {
-            int ok = 1;
-            const int b = blockIdx.x;
-            const int lo = b - R < 0 ? 0 : b - R;
-            const int hi = b + R >= (int)nb ? (int)nb - 1 : b + R;
-            const uint64_t t0 = globaltimer();
-            for (int j = lo; j <= hi && ok; ++j) {
-                if (j == b) continue;
-                unsigned spins = 0;
-                while (ld_acquire_u32(prog + j) < phase) {
-                    if (*(volatile int*)&bar->error) { ok = 0; break; }
-                    if ((++spins & 255u) == 0u && globaltimer() - t0 > kBarrierTimeoutNs) {
-                        atomicExch(&bar->error, 1);
-                        ok = 0;
-                        break;
-                    }
-                    __nanosleep(32);
-                }
-            }
-            __threadfence();
-            s_ok = ok;
-        }
-        __syncthreads();
-        return s_ok != 0;
-    }
-
-    __device__ __forceinline__ bool global_keep_phase() {
-        publish();
-        return grid_sync(bar, nb);
-    }
-
-    __device__ __forceinline__ bool global() {
-        phase += 1;
-        return global_keep_phase();
-    }
-};
-
-// neighbour radius in blocks for chunks of `chunk` compact cells
-__host__ __device__ inline int neighbour_radius(long long SX, long long chunk, unsigned nb) {
-    if (chunk <= 0) return (int)nb;
-    long long r = (SX + 2 + chunk - 1) / chunk + 1;
-    return r >= (long long)nb ? (int)nb : (int)r;
-}
-
 // ---------------------------------------------------------- block reduces
 template <int NT>
 __device__ __forceinline__ double block_sum(double v, double* sh) {

@@ -42,15 +42,6 @@ constexpr int kSweepMinBlocks = TSE_SWEEP_MINB;
 #define TSE_SWEEP_BLOCK 256
 #endif
 constexpr int kSweepBlock = TSE_SWEEP_BLOCK;
-#ifndef TSE_SWEEP_CHUNKED
-#define TSE_SWEEP_CHUNKED 0   // 1: contiguous chunks with neighbour-only phase sync
-#endif
-#ifndef TSE_TMA_ROUNDSYNC
-#define TSE_TMA_ROUNDSYNC 0  // 1: colour phases ordered per round of chunks, device-wide
-                             // barrier only before a check's sums (measured 2.7x slower:
-                             // the GPU-scope release/acquire per chunk sits on the
-                             // critical path)
-#endif
 #ifndef TSE_TMA_PREFETCH
 #define TSE_TMA_PREFETCH 1   // 1: a phase's own parts are copied before its grid barrier
 #endif
@@ -149,18 +140,9 @@ __global__ void __launch_bounds__(kSweepBlock, kSweepMinBlocks) dc_sweep_kernel(
     const long long Nc = c.L.Nc, N = c.Ncal, SX = c.L.SX;
     const int H = c.L.H;
     const int lane = threadIdx.x & 31;
-#if TSE_SWEEP_CHUNKED
-    // contiguous chunk per block, colour phases ordered by neighbour flags
-    const long long chunk0 = (long long)blockIdx.x * c.chunk;
-    const long long end = chunk0 + c.chunk < Nc ? chunk0 + c.chunk : Nc;
-    const long long step = blockDim.x;
-    const long long w0 = chunk0 + threadIdx.x - lane;
-    PhaseSync sync{c.bar, c.prog, nb, c.R, 0u};
-#else
     const long long end = Nc;
     const long long step = (long long)nb * blockDim.x;
     const long long w0 = (long long)blockIdx.x * blockDim.x + threadIdx.x - lane;
-#endif
     const bool leader = (blockIdx.x == 0 && threadIdx.x == 0);
     const float sor = c.sor;
     DcState* st = c.st;
@@ -209,11 +191,7 @@ __global__ void __launch_bounds__(kSweepBlock, kSweepMinBlocks) dc_sweep_kernel(
                     c.partials[4 * blockIdx.x + 2 * (checkno & 1) + 1] = b3;
                 }
             }
-#if TSE_SWEEP_CHUNKED
-            ok = (col == 1 && check) ? sync.global() : sync.local();
-#else
             ok = grid_sync(c.bar, nb);
-#endif
         }
         if (!ok) { event = EV_ERROR; break; }
         diff = 1e100;
@@ -261,44 +239,6 @@ __global__ void __launch_bounds__(kSweepBlock, kSweepMinBlocks) dc_sweep_kernel(
 
 // ------------------------------------------------ FP32 sweeps, TMA-staged
 // (the staging pieces are in tse_dc.cuh)
-// Rounds.  Chunk q = r nb + b is block b's chunk of round r, so a round is a
-// contiguous range of nb chunks, and a chunk's windows reach at most
-// SX + H + 16 cells beyond it: rounds r - delta .. r + delta.  When the
-// consumers of a chunk have written it and released its stage, the producer
-// (which waits for that release anyway) adds 1 to the round's counter
-// (release, GPU scope); before copying a chunk's windows in the next colour
-// phase it makes sure those rounds of the previous phase are complete
-// (acquire, bounded) -- every write it reads is then done, and so is every
-// read of the cells it is about to overwrite.  At a phase end the producer
-// posts all of the phase's chunks, so no round waits for a later phase.  The
-// device-wide barrier remains only before a check's sums.
-
-// producer: advance `ready` (every round <= ready has completed `phases`
-// phases, one post per chunk) until it reaches `need`; false on the block's
-// error flag or after kBarrierTimeoutNs, raising the flag
-__device__ __forceinline__ bool rounds_ready(const unsigned* cnt, long long& ready, long long need,
-                                             long long nch, unsigned nb, unsigned phases,
-                                             volatile int* err) {
-    uint64_t t0 = 0;
-    unsigned spins = 0;
-    while (ready < need) {
-        const long long q = ready + 1;
-        const long long in_round = (nch - q * nb) < (long long)nb ? (nch - q * nb) : (long long)nb;
-        if (ld_acquire_u32(cnt + q) >= phases * (unsigned)in_round) {
-            ready = q;
-            continue;
-        }
-        if (*err) return false;
-        if (t0 == 0) t0 = globaltimer();
-        if ((++spins & 63u) == 0u && globaltimer() - t0 > kBarrierTimeoutNs) {
-            *err = 1;
-            return false;
-        }
-        __nanosleep(32);
-    }
-    return true;
-}
-
 __global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) dc_sweep_tma_kernel(DcCtl c, TmaStage T) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t full[kTmaStages];
@@ -315,16 +255,8 @@ __global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) dc_sweep_tma_kernel
     const int H = c.L.H;
     const long long nch = (Nc + C - 1) / C;
     const long long mine = nch > (long long)b ? (nch - 1 - b) / nb + 1 : 0;   // chunks of this block
-    const long long R = (nch + nb - 1) / nb;                                   // rounds
-    const long long delta = (SX + H + 16 + (long long)nb * C - 1) / ((long long)nb * C);
-    long long ready = -1;        // producer: rounds known complete for the previous phase
-    unsigned* rounds = c.prog;   // per round: chunks posted, zeroed before the launch
-    unsigned* bar_count = c.prog + (kMaxBlocks - 1);   // count_sync's counter (zeroed too)
-    unsigned bars = 0;           // device-wide barriers passed in this launch
-    unsigned phase = 0;          // colour phases completed in this launch
-    unsigned posted = 0;         // producer: uses posted to their round
-    int stage_round[kTmaStages]; // producer: round of each stage's latest use
-    for (int q = 0; q < kTmaStages; ++q) stage_round[q] = q;
+    unsigned* bar_count = c.prog;   // count_sync's counter, zeroed before the launch
+    unsigned bars = 0;              // device-wide barriers passed in this launch
     const bool leader = (b == 0 && tid == 0);
     const float sor = c.sor;
     const uint64_t keep = l2_evict_last();
@@ -390,44 +322,12 @@ __global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) dc_sweep_tma_kernel
                                 pok = false;
                                 break;
                             }
-#if TSE_TMA_ROUNDSYNC
-                            // the stage's previous chunk is written: post it
-                            if (issued >= (unsigned)kTmaStages && posted <= issued - kTmaStages) {
-                                red_release_add(rounds + stage_round[s], 1u);
-                                posted = issued - kTmaStages + 1;
-                            }
-#endif
                             const long long cnt = (N - m0) < C ? (N - m0) : C;   // % 32 == 0
                             tma_issue_own(c, T, stg, &full[s], Kc, dw, msk, m0, cnt);
                         }
-#if TSE_TMA_ROUNDSYNC
-                        if (phase > 0) {
-                            const long long need = i + delta < R - 1 ? i + delta : R - 1;
-                            if (ready < need) {
-                                if (!rounds_ready(rounds, ready, need, nch, nb, phase, err)) {
-                                    pok = false;
-                                    break;
-                                }
-                                fence_proxy_async();
-                            }
-                        }
-                        stage_round[s] = (int)i;
-#endif
                         tma_issue_windows(c, T, stg, &full[s], dq, m0);
                     }
                     primed = 0;
-#if TSE_TMA_ROUNDSYNC
-                    // post every chunk of this phase once its consumers are done
-                    for (; pok && posted < issued; ++posted) {
-                        const unsigned u = posted;
-                        if (!mbar_wait_flag(&empty[u % kTmaStages], (u / kTmaStages) & 1u, err)) {
-                            pok = false;
-                            break;
-                        }
-                        red_release_add(rounds + stage_round[u % kTmaStages], 1u);
-                    }
-                    ready = -1;   // the next phase checks its rounds afresh
-#endif
 #if TSE_TMA_PREFETCH
                     // the next phase's own parts (records, r', flags, own
                     // correction: nothing another block writes) go out as the
@@ -497,17 +397,11 @@ __global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) dc_sweep_tma_kernel
                         }
                     }
                     // the warp's reads of the stage are done: release it
-#if TSE_TMA_ROUNDSYNC
-                    // and its writes are done: the producer posts them for the
-                    // round once every warp has released the stage
-                    fence_proxy_async();
-#endif
                     __syncwarp();
                     if (lane == 0) mbar_arrive(&empty[s]);
                 }
             }
             uses += (unsigned)mine;
-            phase += 1;
             // this phase's stores are read by the next phase's copies
             fence_proxy_async();
             __syncthreads();
@@ -520,13 +414,7 @@ __global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) dc_sweep_tma_kernel
                     c.partials[4 * b + 2 * (checkno & 1) + 1] = b3;
                 }
             }
-#if TSE_TMA_ROUNDSYNC
-            // between phases the rounds order the blocks; a check's sums
-            // need every block
-            if (col == 1 && check) ok = count_sync(bar_count, ++bars * nb, c.bar);
-#else
             ok = count_sync(bar_count, ++bars * nb, c.bar);
-#endif
         }
         if (!ok) { event = EV_ERROR; break; }
         diff = 1e100;
@@ -624,7 +512,7 @@ __global__ void dc_status_kernel(const DcState* st, TseSolveStatus* s) {
 size_t dc_extra_bytes(const Layout& L) {
     long long Ncal = (L.Nc + 31) & ~31LL;
     return 2 * ((size_t)7 * Ncal + (size_t)dc_delta_len(L, Ncal)) * sizeof(float) +
-           align256(sizeof(DcState)) + align256((size_t)kMaxBlocks * sizeof(unsigned)) + 512;
+           align256(sizeof(DcState)) + 256 + 512;
 }
 
 static int sweep_blocks(long long Nc, int cap) {
@@ -674,11 +562,7 @@ static int tma_blocks(long long Nc, int cap, size_t smem) {
     if (nb > nch) nb = nch;
     if (nb > kMaxBlocks / 2) nb = kMaxBlocks / 2;
     if (cap > 0 && nb > cap) nb = cap;
-    if (nb < 1) nb = 1;
-    // one round counter per nb chunks, plus the barrier counter, in the
-    // kMaxBlocks counters of the workspace
-    if ((nch + nb - 1) / nb >= kMaxBlocks) return 0;
-    return (int)nb;
+    return nb < 1 ? 1 : (int)nb;
 }
 
 template <class Form>
@@ -716,8 +600,6 @@ static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, 
     const size_t tma_smem = (size_t)kTmaStages * T.bytes;
     const int nb_tma = tma_blocks(S.L.Nc, cap, tma_smem);
     const int nb = nb_tma > 0 ? nb_tma : sweep_blocks(S.L.Nc, cap);
-    c.chunk = (S.L.Nc + nb - 1) / nb;
-    c.R = neighbour_radius(S.L.SX, c.chunk, (unsigned)nb);
     dc_scale_kernel<<<gcells, kBlock, 0, stream>>>(S.F, c);
     if (cudaGetLastError() != cudaSuccess) return TSE_ERR_LAUNCH;
     const bool timing = opts && opts->timing;
@@ -737,9 +619,8 @@ static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, 
         dc_x2_kernel<<<1, kBlock, 0, stream>>>(c, (int)rb);
         void* args[] = {(void*)&c};
         void* targs[] = {(void*)&c, (void*)&T};
-        // chunked sweep: PhaseSync counters; staged sweep: round counters
-        if ((TSE_SWEEP_CHUNKED || nb_tma > 0) &&
-            cudaMemsetAsync(c.prog, 0, (size_t)kMaxBlocks * sizeof(unsigned), stream) != cudaSuccess) {
+        // staged sweep: its barrier counter starts at 0
+        if (nb_tma > 0 && cudaMemsetAsync(c.prog, 0, sizeof(unsigned), stream) != cudaSuccess) {
             rc = TSE_ERR_LAUNCH;
             break;
         }

@@ -42,9 +42,7 @@ struct DcCtl {
     double* partials;    // sweep kernel: 4 per block; residual kernel: 1 per block
     GridBarrier* bar;
     DcState* st;
-    long long chunk;     // chunked sweep: compact cells per block
-    int R;               // chunked sweep: PhaseSync neighbour radius
-    unsigned* prog;      // chunked sweep: PhaseSync counters
+    unsigned* prog;      // staged sweep: its barrier counter
 };
 
 // K'_q = k_q / Den of one cell (6 FP32 values, one 24-byte record)
@@ -109,7 +107,7 @@ __device__ __forceinline__ float relax(const Cell& a, const float* dq, long long
 
 // FP32 arrays: per colour 7 * Ncal floats (records + r'), then the
 // correction with margins of G >= SX + 1, then the state record and the
-// PhaseSync counters.  The margins also hold the neighbour windows that the
+// staged sweep's barrier counter.  The margins also hold the neighbour windows that the
 // staged sweep copies for a chunk of up to kDcMaxChunk cells at either end
 // (window starts rounded down to 16 bytes, lengths up to 8 floats longer).
 constexpr int kDcMaxChunk = 1024;
