@@ -358,6 +358,7 @@ def timed_steps(ctx, sim, steps, clocks=None):
     torch = ctx.torch
     M = sim.M
     cu0 = dict(M.cell_updates)
+    it0 = dict(sim.counters)
     M.timing, M.timed, M.sweep_timed = True, [], []
     launches0 = M.launches
     if clocks:
@@ -389,6 +390,7 @@ def timed_steps(ctx, sim, steps, clocks=None):
             s_ms += sms
             n_s += launches
     return {"ms": ms, "updates": updates, "launches": M.launches - launches0, "clocks": clk,
+            "iterations": {k: sim.counters[k] - it0[k] for k in it0},
             "p_units": p_units, "p_ms": p_ms, "n_p": n_p,
             "s_units": s_units, "s_ms": s_ms, "n_s": n_s}
 
@@ -555,6 +557,11 @@ def main():
             err[n] = float(numpy.max(numpy.abs(x - y)) / max(numpy.max(numpy.abs(y)), 1e-300))
         fp64 = {"value": upd64 / (ms64 / 1e3), "ms_per_step": ms64 / a.steps,
                 "speedup_fp32dc": value / (upd64 / (ms64 / 1e3)),
+                # the plain form's relaxations for the same steps and
+                # tolerances, over the FP32+DC form's time: the rate extra
+                # correction sweeps cannot inflate
+                "fp64_equivalent_rate_of_fp32dc": upd64 / (ms / 1e3),
+                "iterations": {"fp32dc": res["iterations"], "fp64": r64["iterations"]},
                 "step_time_ratio": (ms64 / a.steps) / (ms / a.steps),
                 "max_rel_err_vs_fp64": err,
                 "roofline": roofline(r64, "fp64", peak, peak_kind)}

@@ -97,6 +97,44 @@ __device__ __forceinline__ bool grid_sync(GridBarrier* b, unsigned nblocks,
     return s_ok != 0;
 }
 
+__device__ __forceinline__ void red_release_add(unsigned* p, unsigned v) {
+    asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Device-wide barrier of the staged and fused sweeps: each block adds 1 to a counter
+// that is zeroed before the launch and never reset in it (release, no value
+// returned), and barrier k of the launch is passed once the counter reaches
+// k * nb (acquire).  No returning atomic, reset or generation flip sits
+// between the last arrival and the waiters' release.  Bounded like
+// grid_sync: on timeout (or another block's error) the error flag is raised
+// and false returned.
+__device__ __forceinline__ bool count_sync(unsigned* counter, unsigned target, GridBarrier* bar,
+                                           unsigned long long timeout_ns = kBarrierTimeoutNs) {
+    __syncthreads();
+    __shared__ int s_ok;
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        red_release_add(counter, 1u);
+        // wrap-safe: blocks are never more than one barrier apart
+        if ((int)(ld_acquire_u32(counter) - target) < 0) {
+            const uint64_t t0 = globaltimer();
+            unsigned spins = 0;
+            while ((int)(ld_acquire_u32(counter) - target) < 0) {
+                if (*(volatile int*)&bar->error) { ok = 0; break; }
+                if ((++spins & 255u) == 0u && globaltimer() - t0 > timeout_ns) {
+                    atomicExch(&bar->error, 1);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
 // ---------------------------------------------------------- block reduces
 template <int NT>
 __device__ __forceinline__ double block_sum(double v, double* sh) {
