@@ -346,6 +346,15 @@ int32_t tse_mass_totals(const TseGrid *grid, const double *phi,
 int32_t tse_selftest_bounded_waits(int32_t *d_result, double timeout_s, void *d_ws,
                                    size_t ws_bytes, void *stream);
 
+/* Sweep kernel of the FP64 solves (tse_compute_P / _C / _T and the no-alloc
+ * pressure solve; no counterpart in the reference): 1 (default) = the staged
+ * kernel (bulk asynchronous copies into shared-memory stages, warp-specialized)
+ * wherever its stages fit, 0 = plain loads.  Both give the same per-cell
+ * values; only the grouping of the convergence check's sums differs.  Applies
+ * to calls launched after it, from any host thread.  Returns the previous
+ * mode, or TSE_ERR_ARG for a mode other than 0 or 1. */
+int32_t tse_set_exact_sweep(int32_t mode);
+
 /* Library version string. */
 const char *tse_version(void);
 

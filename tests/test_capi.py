@@ -107,3 +107,17 @@ def test_selftest_validates_without_gpu():
     assert L.tse_selftest_bounded_waits(None, 0.1, None, 0, None) == -1
     assert L.tse_selftest_bounded_waits(ct.c_void_p(16), 0.1, ct.c_void_p(4096), 100, None) == -1
     assert L.tse_selftest_bounded_waits(ct.c_void_p(16), 0.0, ct.c_void_p(4096), 512, None) == -1
+
+
+def test_exact_sweep_mode_switch_without_gpu():
+    """The FP64 sweep selector takes 0 or 1, returns the previous mode and
+    refuses anything else (no device call)."""
+    L = N.lib()
+    prev = L.tse_set_exact_sweep(0)
+    try:
+        assert prev in (0, 1)
+        assert L.tse_set_exact_sweep(1) == 0
+        assert L.tse_set_exact_sweep(1) == 1
+        assert L.tse_set_exact_sweep(2) == -1 and L.tse_set_exact_sweep(-1) == -1
+    finally:
+        L.tse_set_exact_sweep(prev)

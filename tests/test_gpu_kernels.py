@@ -149,3 +149,52 @@ def test_mass_totals_vs_numpy(cuda_device):
         assert abs(last["species"][s] - species[s]) <= 1e-12 * abs(species[s])
     assert abs(last["heat"] - heat) <= 1e-12 * abs(heat)
     assert len(sim.mass_log) == 2
+
+
+@pytest.mark.parametrize("shape", [(64, 48, 40), (37, 23, 51), (96, 96, 64)])
+def test_staged_and_plain_exact_solves_agree(shape, cuda_device):
+    """The staged FP64 sweep (bulk copies into shared-memory stages) and the
+    plain-load sweep compute every cell with the same operations: over whole
+    pressure and species solves (x and z buoyancy, omega < 1, the IMBLFLO
+    term) their fields agree bit for bit and their iteration counts and dt
+    match."""
+    from transportse_b200 import _native
+    lib = _native.lib()
+    cfg, rng = _random_case(shape, 7)
+    shp = shape
+    K = 1e-12 * numpy.exp(rng.standard_normal(shp))
+    f = dict(c_f=4.5e-10 * rng.uniform(0.5, 1.5, shp), nue=rng.uniform(8e-4, 1.2e-3, shp),
+             rho_f=rng.uniform(995, 1150, shp), phi=rng.uniform(0.05, 0.3, shp))
+    from transportse_b200 import workloads
+    P = workloads.hydrostatic(cfg) + rng.uniform(-300, 300, shp)
+    BP = (rng.uniform(size=shp) < 0.05).astype(float)
+    WP = numpy.where(rng.uniform(size=shp) < 0.2, rng.uniform(-1e-4, 1e-4, shp), 0.0)
+    z = numpy.zeros(shp)
+    C = rng.uniform(0, 1, shp)
+    D = 1e-6 * rng.uniform(0.5, 1.5, shp)
+    BC = (rng.uniform(size=shp) < 0.05).astype(float)
+    WC = numpy.where(rng.uniform(size=shp) < 0.2, 1e-5, 0.0)
+    e = rng.uniform(-1e-6, 1e-6, shp)
+    q = [rng.uniform(-1e-4, 1e-4, shp) for _ in range(3)]
+    m = model_for(cfg, cuda_device)
+    nk = NumpyKernels(m)
+    out = {}
+    prev = lib.tse_set_exact_sweep(1)
+    try:
+        for mode in (1, 0):
+            assert lib.tse_set_exact_sweep(mode) in (0, 1)
+            rp = nk.compute_P(P.copy(), f["c_f"], f["nue"], f["rho_f"], f["phi"], K, K * 0.7, K * 0.2,
+                              z, z, z, 3600.0, BP, WP, SOR=1.7, max_it=20000, inc_it=1.25,
+                              max_dt=1e5, min_dt=1e-8, P_conv=1e-10)
+            rc = [nk.compute_C(C.copy(), D, D, D, f["phi"], f["rho_f"], *q, 3600.0, BC, WC,
+                               numpy.ones(shp), e, omega=om, SOR=1.1, max_it=100, inc_it=1.05,
+                               max_dt=1e5, min_dt=1e-8, C_conv=1e-12) for om in (1, 0.5)]
+            out[mode] = (rp, rc)
+    finally:
+        lib.tse_set_exact_sweep(prev)
+    (p1, c1), (p0, c0) = out[1], out[0]
+    assert p1[5] > 20 and (p1[0], p1[1], p1[4], p1[5]) == (p0[0], p0[1], p0[4], p0[5])
+    assert numpy.array_equal(p1[2], p0[2])
+    for a, b in zip(c1, c0):
+        assert (a[0], a[1], a[3], a[4]) == (b[0], b[1], b[3], b[4])
+        assert numpy.array_equal(a[2], b[2])

@@ -242,6 +242,102 @@ def test_staged_sweep_copies_stay_aligned_and_in_bounds():
         assert _staged_copies_ok(nx, ny, nz, Hmax), (nx, ny, nz, "fused")
 
 
+def _exact_staged_ok(nx, ny, nz, nst, count, sol, C=256):
+    """Every bulk copy of the staged FP64 solve (tse_rbsolve_tma.cuh x_plan,
+    the producer's copies and x_window's clamping) is 16-byte aligned in
+    global and shared memory, a multiple of 16 bytes, inside its array and
+    its stage slot; every shared-memory index a consumer forms stays inside
+    its window; and every neighbour a set flag lets a cell read lies in the
+    copied part of its window.  count: arrays per colour of the form (17
+    pressure, 15 transport), sol: the solution's array index."""
+    nzp = nz + (nz & 1)
+    H = nzp // 2
+    SX = ny * H
+    Nc = nx * SX
+    N = (Nc + 31) & ~31
+    al = lambda b: (b + 255) & ~255
+    # workspace carve of setup_pressure / setup_transport (byte offsets)
+    ws = 256 * 3
+    mask = [ws + al(16) + al(2 * 16384 * 8), 0]
+    mask[1] = mask[0] + al(N)
+    arr = [mask[1] + al(N), 0]
+    arr[1] = arr[0] + 8 * count * N
+    ws_end = arr[1] + 8 * count * N
+    X = [arr[0] + 8 * sol * N, arr[1] + 8 * sol * N]
+    # x_plan
+    xo = nst * C * 8
+    msk = xo + C * 8
+    wz = msk + C
+    lz, lx = C + 2 * H + 2, C + 2
+    wxp, wxm = wz + 8 * lz, wz + 8 * lz + 8 * lx
+    nbytes = (wz + 8 * lz + 16 * lx + 127) & ~127
+
+    def clamp(s, n):
+        a, e = max(s, 0), min(s + n, N)
+        return (a, e) if e > a else None
+
+    for col in (0, 1):
+        for q in range((Nc + C - 1) // C):
+            m0 = q * C
+            cnt = min(C, N - m0)
+            if cnt % 32:
+                return False
+            zs, xps, xms = (m0 - H) & ~1, (m0 + SX) & ~1, (m0 - SX) & ~1
+            # (global address, bytes, array lo, array hi, smem offset, smem slot end)
+            copies = [(arr[col] + 8 * (k * N + m0), 8 * cnt, arr[col] + 8 * k * N,
+                       arr[col] + 8 * (k + 1) * N, 8 * C * k, 8 * C * (k + 1)) for k in range(nst)]
+            copies.append((X[col] + 8 * m0, 8 * cnt, X[col], X[col] + 8 * N, xo, msk))
+            copies.append((mask[col] + m0, cnt, mask[col], mask[col] + N, msk, wz))
+            win = {}
+            for name, s0, n, off in (("z", zs, lz, wz), ("xp", xps, lx, wxp), ("xm", xms, lx, wxm)):
+                r = clamp(s0, n)
+                win[name] = (s0, r)
+                if r:
+                    a, e = r
+                    copies.append((X[1 - col] + 8 * a, 8 * (e - a), X[1 - col], X[1 - col] + 8 * N,
+                                   off + 8 * (a - s0), off + 8 * n))
+            for g, n, lo, hi, d, dend in copies:
+                if g % 16 or n % 16 or d % 16 or g < lo or g + n > hi or hi > ws_end:
+                    return False
+                if d + n > dend or dend > nbytes:
+                    return False
+            oz, oxp, oxm = m0 - zs, m0 + SX - xps, m0 - SX - xms
+            for l in range(min(C, Nc - m0)):
+                m = m0 + l
+                i, j = divmod(m // H, ny)
+                k = 2 * (m % H) + ((col + i + j) & 1)
+                zo = k & 1
+                iz = l + oz
+                idx = [("xp", l + oxp, lx), ("xm", l + oxm, lx), ("z", iz + H, lz),
+                       ("z", iz - H, lz), ("z", iz + zo, lz), ("z", iz - 1 + zo, lz)]
+                for _, ix, n in idx:
+                    if not 0 <= ix < n:
+                        return False
+                if k >= nz:
+                    continue
+                exists = [i < nx - 1, i > 0, j < ny - 1, j > 0, k < nz - 1, k > 0]
+                off = [SX, -SX, H, -H, zo, zo - 1]
+                for e, (name, ix, _), o in zip(exists, idx, off):
+                    if not e:
+                        continue
+                    s0, r = win[name]
+                    if r is None or not (r[0] <= m + o < r[1]) or s0 + ix != m + o:
+                        return False
+    return True
+
+
+def test_exact_staged_copies_stay_aligned_and_in_bounds():
+    import random
+    rng = random.Random(11)
+    shapes = [(1, 1, 1), (1, 1, 2), (2, 1, 1), (3, 3, 3), (1, 1, 40), (9, 1, 31), (5, 7, 3),
+              (60, 1, 30), (33, 17, 21), (2, 2, 600), (60, 40, 2), (24, 24, 20), (7, 3, 257)]
+    shapes += [(rng.randint(1, 24), rng.randint(1, 24), rng.randint(1, 120)) for _ in range(40)]
+    for nx, ny, nz in shapes:
+        for nst, count, sol in ((9, 17, 16), (11, 17, 16), (13, 17, 16),   # pressure
+                                (9, 15, 14), (11, 15, 14)):                # transport
+            assert _exact_staged_ok(nx, ny, nz, nst, count, sol), (nx, ny, nz, nst)
+
+
 def test_server_cancels_pending_requests():
     """A request that has not started can be withdrawn; the others stay queued."""
     from transportse_b200 import workloads

@@ -124,6 +124,7 @@ SIGNATURES = {
     "tse_mass_totals": (_I, [_G, _P, _P, _P, _PP, _PP, _I, _P, _P, _P, _P, _P, _P, _P, _P, _S,
                              _P]),
     "tse_selftest_bounded_waits": (_I, [_P, _D, _P, _S, _P]),
+    "tse_set_exact_sweep": (_I, [_I]),
     "tse_version": (ct.c_char_p, []),
 }
 

@@ -10,6 +10,12 @@
 
 namespace tse {
 
+// offset of neighbour q (x+, x-, y+, y-, z+, z-) of a compact cell in the
+// other colour's array; zo = 1 for cells with odd k
+__device__ __forceinline__ long long nb_offset(int q, long long SX, long long H, long long zo) {
+    return q == 0 ? SX : q == 1 ? -SX : q == 2 ? H : q == 3 ? -H : q == 4 ? zo : zo - 1;
+}
+
 enum PArr {
     PA_A = 0, PA_C, PA_E, PA_G, PA_I, PA_K,   // transmissibilities x+ x- y+ y- z+ z-
     PA_AB, PA_CD, PA_IJ, PA_KL,               // buoyancy products
@@ -28,24 +34,45 @@ struct PressureForm {
 
     __device__ __forceinline__ const double* a(int col, int k) const { return arr[col] + (long long)k * Ncal; }
 
-    // numerator of the update (tse.py:691-694), in the reference's order
-    __device__ __forceinline__ double sum(int col, long long m, uint8_t f, const double* Xo) const {
-        const double* b = arr[col];
-        double s = (f & F_XP) ? b[PA_A * Ncal + m] * __ldcg(Xo + m + SX) : 0.0;
-        s = s + (xgrav ? b[PA_AB * Ncal + m] : 0.0);
-        s = s + ((f & F_XM) ? b[PA_C * Ncal + m] * __ldcg(Xo + m - SX) : 0.0);
-        s = s - (xgrav ? b[PA_CD * Ncal + m] : 0.0);
-        s = s + ((f & F_YP) ? b[PA_E * Ncal + m] * __ldcg(Xo + m + H) : 0.0);
-        s = s + ((f & F_YM) ? b[PA_G * Ncal + m] * __ldcg(Xo + m - H) : 0.0);
-        const long long zo = (long long)(f >> 7);
-        s = s + ((f & F_ZP) ? b[PA_I * Ncal + m] * __ldcg(Xo + m + zo) : 0.0);
-        s = s + (zgrav ? b[PA_IJ * Ncal + m] : 0.0);
-        s = s + ((f & F_ZM) ? b[PA_K * Ncal + m] * __ldcg(Xo + m - 1 + zo) : 0.0);
-        s = s - (zgrav ? b[PA_KL * Ncal + m] : 0.0);
-        s = s + b[PA_RPN * Ncal + m];
-        s = s + b[PA_WP * Ncal + m];
+    // numerator of the update (tse.py:691-694), in the reference's order;
+    // a(k) is coefficient array k of the cell, x(q) its neighbour q (x+, x-,
+    // y+, y-, z+, z-), read only where the flag says the neighbour exists
+    template <class A, class X>
+    __device__ __forceinline__ double sum_with(A a, X x, uint8_t f) const {
+        double s = (f & F_XP) ? a(PA_A) * x(0) : 0.0;
+        s = s + (xgrav ? a(PA_AB) : 0.0);
+        s = s + ((f & F_XM) ? a(PA_C) * x(1) : 0.0);
+        s = s - (xgrav ? a(PA_CD) : 0.0);
+        s = s + ((f & F_YP) ? a(PA_E) * x(2) : 0.0);
+        s = s + ((f & F_YM) ? a(PA_G) * x(3) : 0.0);
+        s = s + ((f & F_ZP) ? a(PA_I) * x(4) : 0.0);
+        s = s + (zgrav ? a(PA_IJ) : 0.0);
+        s = s + ((f & F_ZM) ? a(PA_K) * x(5) : 0.0);
+        s = s - (zgrav ? a(PA_KL) : 0.0);
+        s = s + a(PA_RPN);
+        s = s + a(PA_WP);
         return s;
     }
+    __device__ __forceinline__ double sum(int col, long long m, uint8_t f, const double* Xo) const {
+        const double* b = arr[col];
+        const long long N = Ncal, sx = SX, h = H, zo = (long long)(f >> 7);
+        return sum_with([&](int k) { return b[k * N + m]; },
+                        [&](int q) { return __ldcg(Xo + m + nb_offset(q, sx, h, zo)); }, f);
+    }
+    // the arrays sum_with reads, in a fixed order (host side)
+    int staged_arrays(int* idx) const {
+        int n = 0;
+        const int base[6] = {PA_A, PA_C, PA_E, PA_G, PA_I, PA_K};
+        for (int q = 0; q < 6; ++q) idx[n++] = base[q];
+        if (xgrav) { idx[n++] = PA_AB; idx[n++] = PA_CD; }
+        if (zgrav) { idx[n++] = PA_IJ; idx[n++] = PA_KL; }
+        idx[n++] = PA_RPN;
+        idx[n++] = PA_WP;
+        idx[n++] = PA_DEN;
+        return n;
+    }
+    static constexpr int kSolution = PA_P;
+    static constexpr int kArrays = PA_COUNT;
     __device__ __forceinline__ double den(int col, long long m) const {
         return arr[col][PA_DEN * Ncal + m];
     }
@@ -57,6 +84,11 @@ struct PressureForm {
                                              const double* Xo) const {
         const double s = sum(col, m, f, Xo);
         return (1.0 - SOR) * xold + (SOR * s) / den(col, m);
+    }
+    template <class A, class X>
+    __device__ __forceinline__ double update_with(A a, X x, uint8_t f, double xold) const {
+        const double s = sum_with(a, x, f);
+        return (1.0 - SOR) * xold + (SOR * s) / a(PA_DEN);
     }
 
     // dt halving: P = Pn (tse.py:738) and the dt-dependent R terms
@@ -86,23 +118,41 @@ struct TransportForm {
     int useY, useEX;
     double omega, SOR;
 
-    // numerator of the update (tse.py:870-874), in the reference's order
-    __device__ __forceinline__ double sum(int col, long long m, uint8_t f, const double* Xo) const {
-        const double* b = arr[col];
-        const long long zo = (long long)(f >> 7);
-        double s = (f & F_XP) ? b[TA_A * Ncal + m] * __ldcg(Xo + m + SX) : 0.0;
-        s = s + ((f & F_XM) ? b[TA_B * Ncal + m] * __ldcg(Xo + m - SX) : 0.0);
-        s = s + ((f & F_YP) ? b[TA_C * Ncal + m] * __ldcg(Xo + m + H) : 0.0);
-        s = s + ((f & F_YM) ? b[TA_D * Ncal + m] * __ldcg(Xo + m - H) : 0.0);
-        s = s + ((f & F_ZP) ? b[TA_E * Ncal + m] * __ldcg(Xo + m + zo) : 0.0);
-        s = s + ((f & F_ZM) ? b[TA_F * Ncal + m] * __ldcg(Xo + m - 1 + zo) : 0.0);
+    // numerator of the update (tse.py:870-874), in the reference's order;
+    // a(k) and x(q) as in PressureForm::sum_with
+    template <class A, class X>
+    __device__ __forceinline__ double sum_with(A a, X x, uint8_t f) const {
+        double s = (f & F_XP) ? a(TA_A) * x(0) : 0.0;
+        s = s + ((f & F_XM) ? a(TA_B) * x(1) : 0.0);
+        s = s + ((f & F_YP) ? a(TA_C) * x(2) : 0.0);
+        s = s + ((f & F_YM) ? a(TA_D) * x(3) : 0.0);
+        s = s + ((f & F_ZP) ? a(TA_E) * x(4) : 0.0);
+        s = s + ((f & F_ZM) ? a(TA_F) * x(5) : 0.0);
         double num = omega * s;
-        if (useY) num = num + b[TA_Y * Ncal + m];
-        num = num + b[TA_RXN * Ncal + m];
-        num = num + b[TA_W * Ncal + m];
-        num = num - (useEX ? b[TA_EX * Ncal + m] : 0.0);
+        if (useY) num = num + a(TA_Y);
+        num = num + a(TA_RXN);
+        num = num + a(TA_W);
+        num = num - (useEX ? a(TA_EX) : 0.0);
         return num;
     }
+    __device__ __forceinline__ double sum(int col, long long m, uint8_t f, const double* Xo) const {
+        const double* b = arr[col];
+        const long long N = Ncal, sx = SX, h = H, zo = (long long)(f >> 7);
+        return sum_with([&](int k) { return b[k * N + m]; },
+                        [&](int q) { return __ldcg(Xo + m + nb_offset(q, sx, h, zo)); }, f);
+    }
+    int staged_arrays(int* idx) const {
+        int n = 0;
+        for (int q = 0; q < 6; ++q) idx[n++] = TA_A + q;
+        if (useY) idx[n++] = TA_Y;
+        idx[n++] = TA_RXN;
+        idx[n++] = TA_W;
+        if (useEX) idx[n++] = TA_EX;
+        idx[n++] = TA_DEN;
+        return n;
+    }
+    static constexpr int kSolution = TA_X;
+    static constexpr int kArrays = TA_COUNT;
     __device__ __forceinline__ double den(int col, long long m) const {
         return arr[col][TA_DEN * Ncal + m];
     }
@@ -114,6 +164,11 @@ struct TransportForm {
                                              const double* Xo) const {
         const double num = sum(col, m, f, Xo);
         return (1.0 - SOR) * xold + (SOR * num) / den(col, m);
+    }
+    template <class A, class X>
+    __device__ __forceinline__ double update_with(A a, X x, uint8_t f, double xold) const {
+        const double num = sum_with(a, x, f);
+        return (1.0 - SOR) * xold + (SOR * num) / a(TA_DEN);
     }
 
     // dt halving: X = Xn (tse.py:911, 1077) and the dt-dependent R terms

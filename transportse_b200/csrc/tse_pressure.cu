@@ -14,6 +14,7 @@
 
 #include "tse_forms.cuh"
 #include "tse_rbsolve.cuh"
+#include "tse_rbsolve_tma.cuh"
 
 namespace tse {
 
@@ -210,7 +211,8 @@ extern "C" int32_t tse_compute_P(const TseGrid* grid, const TsePressureArgs* arg
     ctl.partials = S.partials;
     ctl.bar = S.bar;
     ctl.status = d_status;
-    rc = launch_rb_solve(S.F, ctl, stream);
+    rc = launch_rb_solve_tma(S.F, ctl, stream);
+    if (rc == 1) rc = launch_rb_solve(S.F, ctl, stream);
     if (rc != TSE_OK) return rc;
     return launch_unpack(args->P, ctl.X[0], ctl.X[1], L, stream);
 }

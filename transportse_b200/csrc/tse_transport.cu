@@ -11,6 +11,7 @@
 // (tse.py:870-875, 1038-1043) term by term.  Compiled with --fmad=false.
 #include "tse_forms.cuh"
 #include "tse_rbsolve.cuh"
+#include "tse_rbsolve_tma.cuh"
 
 namespace tse {
 
@@ -443,7 +444,8 @@ static int run_transport(const TseGrid* grid, const Args* a, double* X, TseSolve
     ctl.partials = w.partials;
     ctl.bar = w.bar;
     ctl.status = d_status;
-    rc = launch_rb_solve(F, ctl, stream);
+    rc = launch_rb_solve_tma(F, ctl, stream);
+    if (rc == 1) rc = launch_rb_solve(F, ctl, stream);
     if (rc != TSE_OK) return rc;
     const long long nat = (long long)L.nx * L.ny * L.nz;
     unpack_t_kernel<<<(unsigned)((nat + kBlock - 1) / kBlock), kBlock, 0, stream>>>(X, ctl.X[0],
