@@ -47,6 +47,26 @@ constexpr int kSweepBlock = TSE_SWEEP_BLOCK;
 #endif
 constexpr int kResBlocks = 2048;   // fixed grid of the residual kernel (deterministic sums)
 
+// Pipelines of the staged sweep: each has its own producer warp, its own ring
+// of stages and its own consumer groups, and takes every kDcPipes-th
+// chunk of the block.  A producer warp issues its copies one after another,
+// at a rate that bounds a pipeline's throughput; more pipelines per SM (more
+// blocks, or more per block) raise that bound.
+#ifndef TSE_DC_PIPES
+#define TSE_DC_PIPES 2
+#endif
+#ifndef TSE_DC_MINB
+#define TSE_DC_MINB 1                // blocks per SM
+#endif
+#ifndef TSE_DC_STAGES
+#define TSE_DC_STAGES 8              // over all pipelines
+#endif
+constexpr int kDcPipes = TSE_DC_PIPES;
+constexpr int kDcStages = TSE_DC_STAGES;     // at most; fewer where long columns make stages big
+constexpr int kDcThreads = kTmaConsumers + 32 * kDcPipes;
+static_assert(kDcStages % kDcPipes == 0 && kDcStages >= 2 * kDcPipes, "two or more stages a ring");
+static_assert((kTmaConsumers / kTmaGroup) % kDcPipes == 0, "every pipeline has its own consumer groups");
+
 // ------------------------------------------------------------ FP64 kernels
 // K'_q = k_q / Den for every cell (at the start and after dt halving)
 template <class Form>
@@ -239,22 +259,32 @@ __global__ void __launch_bounds__(kSweepBlock, kSweepMinBlocks) dc_sweep_kernel(
 
 // ------------------------------------------------ FP32 sweeps, TMA-staged
 // (the staging pieces are in tse_dc.cuh)
-__global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) dc_sweep_tma_kernel(DcCtl c, TmaStage T) {
+template <int RING>
+__global__ void __launch_bounds__(kDcThreads, TSE_DC_MINB) dc_sweep_tma_kernel(DcCtl c, TmaStage T) {
     extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ __align__(8) uint64_t full[kTmaStages];
-    __shared__ __align__(8) uint64_t empty[kTmaStages];
-    __shared__ double sh[kTmaThreads / 32];
+    __shared__ __align__(8) uint64_t full[kDcStages];
+    __shared__ __align__(8) uint64_t empty[kDcStages];
+    __shared__ double sh[kDcThreads / 32];
     __shared__ int s_err;
     const unsigned nb = gridDim.x, b = blockIdx.x;
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
-    const bool producer = warp == kTmaConsumers / 32;
-    const int group = warp >> 2;                        // consumers: 0 or 1
+    const bool producer = warp >= kTmaConsumers / 32;
+    const int group = tid / kTmaGroup;                  // consumers: 0 or 1
     const int gt = tid & (kTmaGroup - 1);               // thread within its group
+    // this thread's pipeline (producer warp + its ring of stages +
+    // its consumer groups), and a consumer group's rank within it
+    const int pipe = producer ? warp - kTmaConsumers / 32 : group % kDcPipes;
+    const int grank = group / kDcPipes;
+    constexpr int kGroupsPerPipe = (kTmaConsumers / kTmaGroup) / kDcPipes;
+    constexpr unsigned ring = RING;                     // stages of a ring (T.stages / kDcPipes)
+    const unsigned ring0 = (unsigned)pipe * ring;    // the pipeline's first stage
     const long long Nc = c.L.Nc, N = c.Ncal, SX = c.L.SX, C = kTmaChunk;
     const int H = c.L.H;
     const long long nch = (Nc + C - 1) / C;
     const long long mine = nch > (long long)b ? (nch - 1 - b) / nb + 1 : 0;   // chunks of this block
+    // this pipeline's chunks of a phase: i = pipe, pipe + kDcPipes, ...
+    const long long pmine = mine > pipe ? (mine - 1 - pipe) / kDcPipes + 1 : 0;
     unsigned* bar_count = c.prog;   // count_sync's counter, zeroed before the launch
     unsigned bars = 0;              // device-wide barriers passed in this launch
     const bool leader = (b == 0 && tid == 0);
@@ -269,26 +299,26 @@ __global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) dc_sweep_tma_kernel
     volatile int* err = &s_err;
 
     if (tid == 0) {
-        for (int s = 0; s < kTmaStages; ++s) {
+        for (int s = 0; s < RING * kDcPipes; ++s) {
             mbar_init(&full[s], 1);
-            mbar_init(&empty[s], kTmaConsumers / 64);   // one arrival per warp of a group
+            mbar_init(&empty[s], kTmaGroup / 32);   // one arrival per warp of a group
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_err = 0;
     }
     __syncthreads();
-    unsigned uses = 0;      // chunks this block has consumed, over all colour phases
-    unsigned issued = 0;    // producer: chunks issued, over all colour phases
+    unsigned uses = 0;      // this pipeline's chunks consumed, over all colour phases
+    unsigned issued = 0;    // producer: this pipeline's chunks issued, over all phases
     // producer: chunks of the coming phase whose own parts are already in flight
     long long primed = 0;
-    const long long pro = mine < kTmaStages ? mine : kTmaStages;
+    const long long pro = pmine < (long long)ring ? pmine : (long long)ring;
 #if TSE_TMA_PREFETCH
     if (producer && lane == 0) {
         for (long long j = 0; j < pro; ++j) {
-            const long long m0 = (b + j * nb) * C;
+            const long long m0 = (b + (pipe + j * kDcPipes) * nb) * C;
             const long long cnt = (N - m0) < C ? (N - m0) : C;
-            tma_issue_own(c, T, smem + (size_t)j * T.bytes, &full[j], c.K[0], c.D[0], c.mask[0], m0,
-                          cnt);
+            tma_issue_own(c, T, smem + (size_t)(ring0 + j) * T.bytes, &full[ring0 + j], c.K[0], c.D[0],
+                          c.mask[0], m0, cnt);
         }
         primed = pro;
     }
@@ -312,13 +342,13 @@ __global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) dc_sweep_tma_kernel
                     // the grid barrier; the copies read it through the async proxy
                     fence_proxy_async();
                     bool pok = true;
-                    for (long long i = 0; i < mine; ++i, ++issued) {
-                        const unsigned s = issued % kTmaStages;
-                        const long long m0 = (b + i * nb) * C;
+                    for (long long j = 0; j < pmine; ++j, ++issued) {
+                        const unsigned s = ring0 + issued % ring;
+                        const long long m0 = (b + (pipe + j * kDcPipes) * nb) * C;
                         unsigned char* stg = smem + (size_t)s * T.bytes;
-                        if (i >= primed) {
-                            if (issued >= (unsigned)kTmaStages &&
-                                !mbar_wait_flag(&empty[s], (issued / kTmaStages - 1) & 1u, err)) {
+                        if (j >= primed) {
+                            if (issued >= (unsigned)ring &&
+                                !mbar_wait_flag(&empty[s], (issued / ring - 1) & 1u, err)) {
                                 pok = false;
                                 break;
                             }
@@ -335,11 +365,11 @@ __global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) dc_sweep_tma_kernel
                     const int nc = 1 - col;
                     for (long long j = 0; pok && j < pro; ++j) {
                         const unsigned v = issued + (unsigned)j;
-                        const unsigned s = v % kTmaStages;
-                        if (v >= (unsigned)kTmaStages &&
-                            !mbar_wait_flag(&empty[s], (v / kTmaStages - 1) & 1u, err))
+                        const unsigned s = ring0 + v % ring;
+                        if (v >= (unsigned)ring &&
+                            !mbar_wait_flag(&empty[s], (v / ring - 1) & 1u, err))
                             break;
-                        const long long m0 = (b + j * nb) * C;
+                        const long long m0 = (b + (pipe + j * kDcPipes) * nb) * C;
                         const long long cnt = (N - m0) < C ? (N - m0) : C;
                         tma_issue_own(c, T, smem + (size_t)s * T.bytes, &full[s], c.K[nc], c.D[nc],
                                       c.mask[nc], m0, cnt);
@@ -349,17 +379,17 @@ __global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) dc_sweep_tma_kernel
                 }
                 __syncwarp();
             } else {
-                for (long long i = group; i < mine; i += 2) {
-                    const unsigned u = uses + (unsigned)i;
-                    const unsigned s = u % kTmaStages;
+                for (long long j = grank; j < pmine; j += kGroupsPerPipe) {
+                    const unsigned u = uses + (unsigned)j;
+                    const unsigned s = ring0 + u % ring;
                     // warp-uniform: lane 0 waits, the warp follows its outcome,
                     // then every lane observes the completed phase (acquire)
                     int okw = 1;
-                    if (lane == 0) okw = mbar_wait_flag(&full[s], (u / kTmaStages) & 1u, err);
+                    if (lane == 0) okw = mbar_wait_flag(&full[s], (u / ring) & 1u, err);
                     if (!__shfl_sync(0xffffffffu, okw, 0)) break;
-                    mbar_try_wait(&full[s], (u / kTmaStages) & 1u);
+                    mbar_try_wait(&full[s], (u / ring) & 1u);
                     const unsigned char* stg = smem + (size_t)s * T.bytes;
-                    const long long m0 = (b + i * nb) * C;
+                    const long long m0 = (b + (pipe + j * kDcPipes) * nb) * C;
                     const int nval = (int)((Nc - m0) < C ? (Nc - m0) : C);
                     // window offsets of cell l of the chunk (32-bit from here on)
                     const int oz = (int)(m0 - ((m0 - H - 1) & ~3LL));
@@ -401,14 +431,14 @@ __global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) dc_sweep_tma_kernel
                     if (lane == 0) mbar_arrive(&empty[s]);
                 }
             }
-            uses += (unsigned)mine;
+            uses += (unsigned)pmine;
             // this phase's stores are read by the next phase's copies
             fence_proxy_async();
             __syncthreads();
             if (*err) { ok = false; break; }   // block-uniform after the barrier
             if (col == 1 && check) {
-                const double b1 = block_sum<kTmaThreads>((double)d2, sh);
-                const double b3 = block_sum<kTmaThreads>((double)dd, sh);
+                const double b1 = block_sum<kDcThreads>((double)d2, sh);
+                const double b3 = block_sum<kDcThreads>((double)dd, sh);
                 if (tid == 0) {
                     c.partials[4 * b + 2 * (checkno & 1)] = b1;
                     c.partials[4 * b + 2 * (checkno & 1) + 1] = b3;
@@ -425,8 +455,8 @@ __global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) dc_sweep_tma_kernel
                 s1 = s1 + __ldcg(c.partials + 4 * q + 2 * (checkno & 1));
                 s3 = s3 + __ldcg(c.partials + 4 * q + 2 * (checkno & 1) + 1);
             }
-            s1 = block_sum<kTmaThreads>(s1, sh);
-            s3 = block_sum<kTmaThreads>(s3, sh);
+            s1 = block_sum<kDcThreads>(s1, sh);
+            s3 = block_sum<kDcThreads>(s3, sh);
             if (tid == 0) {
                 sh[0] = s1;
                 sh[1] = s3;
@@ -466,14 +496,14 @@ __global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) dc_sweep_tma_kernel
         // issued use of each stage; primed stages get their missing arrival
         if (event == EV_ERROR) {
             atomicExch(&c.bar->error, 1);
-            const unsigned first = issued > (unsigned)kTmaStages ? issued - kTmaStages : 0u;
+            const unsigned first = issued > (unsigned)ring ? issued - ring : 0u;
             for (unsigned v = first; v < issued; ++v)
-                mbar_wait_bounded(&full[v % kTmaStages], (v / kTmaStages) & 1u);
+                mbar_wait_bounded(&full[ring0 + v % ring], (v / ring) & 1u);
         }
         for (long long j = 0; j < primed; ++j) {
             const unsigned v = issued + (unsigned)j;
-            mbar_arrive(&full[v % kTmaStages]);
-            mbar_wait_bounded(&full[v % kTmaStages], (v / kTmaStages) & 1u);
+            mbar_arrive(&full[ring0 + v % ring]);
+            mbar_wait_bounded(&full[ring0 + v % ring], (v / ring) & 1u);
         }
     }
     if (leader) {
@@ -537,21 +567,42 @@ static int sweep_blocks(long long Nc, int cap) {
 #ifndef TSE_SWEEP_TMA
 #define TSE_SWEEP_TMA 1   // 1: TMA-staged sweeps where the stages fit in shared memory
 #endif
-constexpr size_t kTmaMaxSmem = 200 * 1024;
+// dynamic shared memory ceiling of the staged sweep: the device's per-block
+// opt-in limit less the kernel's static arrays and a margin
+static size_t tma_max_smem() {
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return optin > 2048 ? (size_t)optin - 2048 : 0;
+}
 
 // blocks of the staged sweep: as many as fit (dynamic shared memory
 // included), at most one per chunk of a colour; 0 when the stages for this
 // grid's windows do not fit (the plain sweep kernel runs instead)
-static int tma_blocks(long long Nc, int cap, size_t smem) {
-    if (!TSE_SWEEP_TMA || smem > kTmaMaxSmem) return 0;
+// the instantiation for a ring of `ring` stages (2 .. kDcStages / kDcPipes)
+static const void* tma_kernel(int ring) {
+    constexpr int kMaxRing = kDcStages / kDcPipes;
+    switch (ring < kMaxRing ? ring : kMaxRing) {
+        case 2: return (const void*)dc_sweep_tma_kernel<2>;
+        case 3: return (const void*)dc_sweep_tma_kernel<(3 <= kMaxRing ? 3 : 2)>;
+        default: return (const void*)dc_sweep_tma_kernel<(4 <= kMaxRing ? 4 : kMaxRing)>;
+    }
+}
+
+static int tma_blocks(long long Nc, int cap, size_t smem, const void* kernel) {
+    const size_t ceil_smem = tma_max_smem();
+    if (!TSE_SWEEP_TMA || smem == 0 || smem > ceil_smem) return 0;
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     // the same ceiling for every grid, so concurrent callers never lower it
     // below another's launch
-    if (cudaFuncSetAttribute(dc_sweep_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)kTmaMaxSmem) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dc_sweep_tma_kernel, kTmaThreads, smem) !=
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ceil_smem) !=
+            cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kDcThreads, smem) !=
             cudaSuccess ||
         per_sm < 1) {
         cudaGetLastError();
@@ -596,9 +647,17 @@ static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, 
         return TSE_ERR_LAUNCH;
     const long long cells2 = 2 * S.L.Nc;
     const unsigned gcells = (unsigned)((cells2 + kBlock - 1) / kBlock);
-    const TmaStage T = tma_stage(S.L.H);
-    const size_t tma_smem = (size_t)kTmaStages * T.bytes;
-    const int nb_tma = tma_blocks(S.L.Nc, cap, tma_smem);
+    TmaStage T = tma_stage(S.L.H);
+    // as many stages as fit, up to kDcStages, an equal ring per pipeline
+    {
+        const size_t cap = tma_max_smem();
+        int st = cap > 0 ? (int)std::min<size_t>((size_t)kDcStages, cap / (size_t)T.bytes) : 0;
+        st -= st % kDcPipes;
+        T.stages = st >= 2 * kDcPipes ? st : 0;
+    }
+    const size_t tma_smem = (size_t)T.stages * T.bytes;
+    const void* tma_k = T.stages > 0 ? tma_kernel(T.stages / kDcPipes) : nullptr;
+    const int nb_tma = tma_k ? tma_blocks(S.L.Nc, cap, tma_smem, tma_k) : 0;
     const int nb = nb_tma > 0 ? nb_tma : sweep_blocks(S.L.Nc, cap);
     dc_scale_kernel<<<gcells, kBlock, 0, stream>>>(S.F, c);
     if (cudaGetLastError() != cudaSuccess) return TSE_ERR_LAUNCH;
@@ -630,8 +689,8 @@ static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, 
             break;
         }
         const cudaError_t le =
-            nb_tma > 0 ? cudaLaunchCooperativeKernel((const void*)dc_sweep_tma_kernel, dim3(nb),
-                                                     dim3(kTmaThreads), targs, tma_smem, stream)
+            nb_tma > 0 ? cudaLaunchCooperativeKernel(tma_k, dim3(nb),
+                                                     dim3(kDcThreads), targs, tma_smem, stream)
                        : cudaLaunchCooperativeKernel((const void*)dc_sweep_kernel, dim3(nb),
                                                      dim3(kSweepBlock), args, 0, stream);
         if (le != cudaSuccess) {

@@ -184,6 +184,7 @@ static_assert(kTmaChunk <= kDcMaxChunk, "windows must stay inside the correction
 struct TmaStage {
     int rec, rp, msk, dw, wz, wxp, wxm, bytes;
     int lz, lx;   // window lengths in floats
+    int stages;   // stages of the launch, over all its pipelines (set by the launcher)
 };
 
 __host__ __device__ inline TmaStage tma_stage(int H) {
@@ -201,6 +202,7 @@ __host__ __device__ inline TmaStage tma_stage(int H) {
     t.wxp = t.wz + 4 * t.lz;
     t.wxm = t.wxp + 4 * t.lx;
     t.bytes = (t.wxm + 4 * t.lx + 127) & ~127;
+    t.stages = kTmaStages;
     return t;
 }
 

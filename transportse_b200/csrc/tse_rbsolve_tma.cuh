@@ -32,19 +32,22 @@ namespace tse {
 #define TSE_X_CHUNK 256
 #endif
 #ifndef TSE_X_MINB
-#define TSE_X_MINB 2          // blocks per SM the shared-memory plan is sized for
+#define TSE_X_MINB 1          // blocks per SM the shared-memory plan is sized for
 #endif
 #ifndef TSE_X_STAGES
-#define TSE_X_STAGES 4        // at most
+#define TSE_X_STAGES 8        // at most, over all pipelines
 #endif
 #ifndef TSE_X_GROUPS
 #define TSE_X_GROUPS 2        // consumer groups, each computing its own chunks
 #endif
 #ifndef TSE_X_PIPES
-#define TSE_X_PIPES 1         // independent pipelines (producer warp + stage ring)
+#define TSE_X_PIPES 2         // independent pipelines (producer warp + stage ring)
 #endif
 constexpr int kXChunk = TSE_X_CHUNK;                  // cells per chunk
-constexpr int kXConsumers = 256;                      // 8 warps
+#ifndef TSE_X_CONSUMERS
+#define TSE_X_CONSUMERS 256   // consumer threads
+#endif
+constexpr int kXConsumers = TSE_X_CONSUMERS;
 constexpr int kXGroups = TSE_X_GROUPS;
 constexpr int kXGroup = kXConsumers / kXGroups;
 // Pipeline r: producer warp r, the consumer groups g with g % kXPipes == r,
@@ -115,7 +118,7 @@ __device__ __forceinline__ void x_window(unsigned char* dst, const double* X, lo
     if (bytes) bulk_g2s_hint(dst + 8 * (a - s), X + a, bytes, bar, policy);
 }
 
-template <class Form>
+template <class Form, int RING>
 __global__ void __launch_bounds__(kXThreads, TSE_X_MINB) rb_solve_tma_kernel(Form F, SolveCtl c, XPlan P) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t full[kXMaxStages];
@@ -136,8 +139,8 @@ __global__ void __launch_bounds__(kXThreads, TSE_X_MINB) rb_solve_tma_kernel(For
     constexpr int kGroupsPerPipe = kXGroups / kXPipes;
     const long long Nc = c.L.Nc, N = c.Ncal, SX = c.L.SX, C = kXChunk;
     const int H = c.L.H;
-    const unsigned S = (unsigned)P.stages;
-    const unsigned Sp = S / kXPipes;                    // stages of a ring
+    constexpr unsigned S = RING * kXPipes;              // P.stages
+    constexpr unsigned Sp = RING;                       // stages of a ring
     const unsigned ring0 = (unsigned)pipe * Sp;         // this pipeline's first stage
     const long long nch = (Nc + C - 1) / C;
     const long long mine = nch > (long long)b ? (nch - 1 - b) / nb + 1 : 0;
@@ -386,17 +389,26 @@ inline int launch_rb_solve_tma(const Form& F, SolveCtl& ctl, cudaStream_t stream
     const int budget = per_sm_smem / TSE_X_MINB - 2048;
     XPlan P;
     if (budget <= 0 || !x_plan(F, ctl.L, budget < optin ? budget : optin, P)) return 1;
-    const int dyn = P.stages * P.bytes;
+    // one instantiation per ring length (2, 3 or 4 stages): stage and parity
+    // arithmetic by compile-time constants
+    constexpr int kMaxRing = kXMaxStages / kXPipes;
+    constexpr int kR3 = kMaxRing < 3 ? 2 : 3, kR4 = kMaxRing < 4 ? kR3 : 4;
+    const int avail = P.stages / kXPipes;
+    const int ring = avail >= kR4 ? kR4 : avail >= kR3 ? kR3 : 2;
+    const void* kernel = ring == kR4   ? (const void*)rb_solve_tma_kernel<Form, kR4>
+                         : ring == kR3 ? (const void*)rb_solve_tma_kernel<Form, kR3>
+                                       : (const void*)rb_solve_tma_kernel<Form, 2>;
+    P.stages = ring * kXPipes;
     // a fixed ceiling, set once per call (no per-size attribute changes that
     // concurrent host threads could interleave)
-    if (cudaFuncSetAttribute(rb_solve_tma_kernel<Form>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              budget < optin ? budget : optin) != cudaSuccess) {
         cudaGetLastError();
         return 1;
     }
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, rb_solve_tma_kernel<Form>, kXThreads,
-                                                      dyn) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kXThreads, P.stages * P.bytes) !=
+            cudaSuccess ||
         per_sm < 1) {
         cudaGetLastError();
         return 1;
@@ -408,9 +420,8 @@ inline int launch_rb_solve_tma(const Form& F, SolveCtl& ctl, cudaStream_t stream
     if (nb < 1) nb = 1;
     if (nb > kMaxBlocks) nb = kMaxBlocks;
     void* args[] = {(void*)&F, (void*)&ctl, (void*)&P};
-    const cudaError_t e = cudaLaunchCooperativeKernel((const void*)rb_solve_tma_kernel<Form>,
-                                                      dim3((unsigned)nb), dim3(kXThreads), args,
-                                                      (size_t)dyn, stream);
+    const cudaError_t e = cudaLaunchCooperativeKernel(kernel, dim3((unsigned)nb), dim3(kXThreads), args,
+                                                      (size_t)P.stages * P.bytes, stream);
     return e == cudaSuccess ? TSE_OK : TSE_ERR_LAUNCH;
 }
 

@@ -42,7 +42,7 @@ from .batch import BatchGate
 from .driver import Simulation
 
 # resident cooperative blocks per SM of the mixed-precision sweep kernel
-SWEEP_BLOCKS_PER_SM = 2   # the staged sweep kernel's residency (dc_sweep_tma_kernel)
+SWEEP_BLOCKS_PER_SM = 1   # the staged sweep kernel's residency (dc_sweep_tma_kernel)
 
 
 def state_bytes(config, precision="fp32dc"):
