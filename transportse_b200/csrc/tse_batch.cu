@@ -329,6 +329,14 @@ static void fill_ctl(DcCtl& c, double inc_it, double max_dt, double min_dt, doub
 static bool finite_dt(double dt, double min_dt) { return std::isfinite(dt) && std::isfinite(min_dt); }
 
 // ====================================================== fused batched sweeps
+// Pipelines of the fused sweep (as in the single-model staged sweep): two
+// producer warps, each with its own ring of stages and consumer group, one
+// block per SM.
+constexpr int kFusedPipes = 2;
+constexpr int kFusedStages = 8;   // at most, over both rings
+constexpr int kFusedThreads = kTmaConsumers + 32 * kFusedPipes;
+static_assert((kTmaConsumers / kTmaGroup) % kFusedPipes == 0, "every pipeline has its own consumer group");
+
 // All models of a batch in one cooperative sweep: the chunks (kTmaChunk
 // cells) of every active model form one table, interleaved over the blocks,
 // and every block runs the staged producer/consumer pipeline of
@@ -423,26 +431,33 @@ __device__ void fused_decide(const FusedItem& I, int g, int num_it, bool check, 
     if (ev != EV_NONE) atomicExch(any_event, 1);
 }
 
-__global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) fused_sweep_kernel(FusedArgs A, TmaStage T) {
+template <int RING>
+__global__ void __launch_bounds__(kFusedThreads, 1) fused_sweep_kernel(FusedArgs A, TmaStage T) {
     extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ __align__(8) uint64_t full[kTmaStages];
-    __shared__ __align__(8) uint64_t empty[kTmaStages];
-    __shared__ double sh[kTmaThreads / 32];
+    __shared__ __align__(8) uint64_t full[RING * kFusedPipes];
+    __shared__ __align__(8) uint64_t empty[RING * kFusedPipes];
+    __shared__ double sh[kFusedThreads / 32];
     __shared__ int s_err;
     const unsigned nb = gridDim.x, b = blockIdx.x;
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
-    const bool producer = warp == kTmaConsumers / 32;
-    const int group = warp >> 2;
+    const bool producer = warp >= kTmaConsumers / 32;
+    const int group = tid / kTmaGroup;                  // consumers: 0 or 1
     const int gt = tid & (kTmaGroup - 1);
+    // pipelines as in dc_sweep_tma_kernel: producer warp + ring + groups
+    const int pipe = producer ? warp - kTmaConsumers / 32 : group % kFusedPipes;
+    const int grank = group / kFusedPipes;
+    constexpr int kGroupsPerPipe = (kTmaConsumers / kTmaGroup) / kFusedPipes;
+    const unsigned ring0 = (unsigned)pipe * RING;
     const long long C = kTmaChunk;
     const long long mine = A.nchunks > (long long)b ? (A.nchunks - 1 - b) / nb + 1 : 0;
+    const long long pmine = mine > pipe ? (mine - 1 - pipe) / kFusedPipes + 1 : 0;
     const uint64_t keep = l2_evict_last();
     volatile int* err = &s_err;
     if (tid == 0) {
-        for (int s = 0; s < kTmaStages; ++s) {
+        for (int s = 0; s < RING * kFusedPipes; ++s) {
             mbar_init(&full[s], 1);
-            mbar_init(&empty[s], kTmaConsumers / 64);
+            mbar_init(&empty[s], kTmaGroup / 32);   // one arrival per warp of a group
         }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         s_err = 0;
@@ -459,12 +474,12 @@ __global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) fused_sweep_kernel(
             if (producer) {
                 if (lane == 0) {
                     fence_proxy_async();
-                    for (long long i = 0; i < mine; ++i, ++issued) {
-                        const unsigned s = issued % kTmaStages;
-                        if (issued >= (unsigned)kTmaStages &&
-                            !mbar_wait_flag(&empty[s], (issued / kTmaStages - 1) & 1u, err))
+                    for (long long j = 0; j < pmine; ++j, ++issued) {
+                        const unsigned s = ring0 + issued % RING;
+                        if (issued >= (unsigned)RING &&
+                            !mbar_wait_flag(&empty[s], (issued / RING - 1) & 1u, err))
                             break;
-                        const FusedChunk ch = A.chunks[b + i * nb];
+                        const FusedChunk ch = A.chunks[b + (pipe + j * kFusedPipes) * nb];
                         const DcCtl& c = A.items[ch.item].c;
                         const long long cnt = (c.Ncal - ch.m0) < C ? (c.Ncal - ch.m0) : C;
                         unsigned char* stg = smem + (size_t)s * T.bytes;
@@ -474,17 +489,17 @@ __global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) fused_sweep_kernel(
                 }
                 __syncwarp();
             } else {
-                for (long long i = group; i < mine; i += 2) {
-                    const unsigned u = uses + (unsigned)i;
-                    const unsigned s = u % kTmaStages;
+                for (long long j = grank; j < pmine; j += kGroupsPerPipe) {
+                    const unsigned u = uses + (unsigned)j;
+                    const unsigned s = ring0 + u % RING;
                     // warp-uniform: lane 0 waits, the warp follows its outcome,
                     // then every lane observes the completed phase (acquire)
                     int okw = 1;
-                    if (lane == 0) okw = mbar_wait_flag(&full[s], (u / kTmaStages) & 1u, err);
+                    if (lane == 0) okw = mbar_wait_flag(&full[s], (u / RING) & 1u, err);
                     if (!__shfl_sync(0xffffffffu, okw, 0)) break;
-                    mbar_try_wait(&full[s], (u / kTmaStages) & 1u);
+                    mbar_try_wait(&full[s], (u / RING) & 1u);
                     const unsigned char* stg = smem + (size_t)s * T.bytes;
-                    const long long q = b + i * nb;
+                    const long long q = b + (pipe + j * kFusedPipes) * nb;
                     const FusedChunk ch = A.chunks[q];
                     const DcCtl& c = A.items[ch.item].c;
                     const long long m0 = ch.m0, SX = c.L.SX;
@@ -542,7 +557,7 @@ __global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) fused_sweep_kernel(
                     }
                 }
             }
-            uses += (unsigned)mine;
+            uses += (unsigned)pmine;
             fence_proxy_async();
             __syncthreads();
             if (*err) { ok = false; break; }
@@ -563,8 +578,8 @@ __global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) fused_sweep_kernel(
                             s3 = s3 + pj.y;
                         }
                     }
-                s1 = block_sum<kTmaThreads>(s1, sh);
-                s3 = block_sum<kTmaThreads>(s3, sh);
+                s1 = block_sum<kFusedThreads>(s1, sh);
+                s3 = block_sum<kFusedThreads>(s3, sh);
                 if (tid == 0) fused_decide(I, g, num_it, check, s1, s3, A.any_event);
                 __syncthreads();
             }
@@ -576,9 +591,9 @@ __global__ void __launch_bounds__(kTmaThreads, TSE_TMA_MINB) fused_sweep_kernel(
         // the last copies issued into each stage land before the block's
         // shared memory is released (bounded waits, flag ignored)
         atomicExch(&A.bar->error, 1);
-        const unsigned first = issued > (unsigned)kTmaStages ? issued - kTmaStages : 0u;
+        const unsigned first = issued > (unsigned)RING ? issued - RING : 0u;
         for (unsigned v = first; v < issued; ++v)
-            mbar_wait_bounded(&full[v % kTmaStages], (v / kTmaStages) & 1u);
+            mbar_wait_bounded(&full[ring0 + v % RING], (v / RING) & 1u);
     }
     if (!ok && b == 0 && tid == 0)
         for (int it = 0; it < A.nitems; ++it) A.items[it].c.st->event = EV_ERROR;
@@ -589,7 +604,17 @@ __global__ void fused_gather_kernel(const FusedItem* items, int n, DcState* out)
     if (i < n) out[i] = *items[i].c.st;
 }
 
-constexpr size_t kFusedMaxSmem = 200 * 1024;
+// dynamic shared memory ceiling: the device's per-block opt-in limit less the
+// kernel's static arrays and a margin
+static size_t fused_max_smem() {
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return optin > 2048 ? (size_t)optin - 2048 : 0;
+}
 
 // bytes of the fused form's batch workspace for n models of `cells` cells in all
 static size_t fused_ws_bytes(int n, long long cells) {
@@ -610,9 +635,19 @@ static int run_fused(std::vector<BatchItem<Form>>& v, TseDcOptions* opts, void* 
         Hmax = it.c.L.H > Hmax ? it.c.L.H : Hmax;
     }
     if (fused_ws_bytes(n, cells) > ws_bytes) return TSE_ERR_WORKSPACE;
-    const TmaStage T = tma_stage(Hmax);
-    const size_t smem = (size_t)kTmaStages * T.bytes;
-    if (smem > kFusedMaxSmem) return TSE_ERR_ARG;
+    TmaStage T = tma_stage(Hmax);
+    // as many stages as fit (up to kFusedStages), an equal ring per pipeline;
+    // one instantiation per ring length
+    const size_t cap_smem = fused_max_smem();
+    int nst = (int)std::min<size_t>((size_t)kFusedStages, cap_smem / (size_t)T.bytes);
+    const int ring = nst / kFusedPipes;
+    if (ring < 2) return TSE_ERR_ARG;
+    const void* kernel = ring >= 4   ? (const void*)fused_sweep_kernel<4>
+                         : ring == 3 ? (const void*)fused_sweep_kernel<3>
+                                     : (const void*)fused_sweep_kernel<2>;
+    nst = (ring >= 4 ? 4 : ring) * kFusedPipes;
+    T.stages = nst;
+    const size_t smem = (size_t)nst * T.bytes;
     // carve the batch workspace
     const size_t nch_max = (size_t)(cells / kTmaChunk) + (size_t)n + 1;
     char* p = (char*)d_ws;
@@ -631,10 +666,9 @@ static int run_fused(std::vector<BatchItem<Form>>& v, TseDcOptions* opts, void* 
     int dev = 0, sms = 0, per_sm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaFuncSetAttribute(fused_sweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)kFusedMaxSmem) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fused_sweep_kernel, kTmaThreads, smem) !=
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap_smem) !=
             cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kFusedThreads, smem) != cudaSuccess ||
         per_sm < 1)
         return TSE_ERR_LAUNCH;
 
@@ -720,8 +754,8 @@ static int run_fused(std::vector<BatchItem<Form>>& v, TseDcOptions* opts, void* 
         }
         void* args[] = {(void*)&A, (void*)&T};
         if (timing) cudaEventRecord(ev0, stream);
-        if (cudaLaunchCooperativeKernel((const void*)fused_sweep_kernel, dim3((unsigned)nb),
-                                        dim3(kTmaThreads), args, smem, stream) != cudaSuccess) {
+        if (cudaLaunchCooperativeKernel(kernel, dim3((unsigned)nb), dim3(kFusedThreads), args, smem,
+                                        stream) != cudaSuccess) {
             rc = TSE_ERR_LAUNCH;
             break;
         }
