@@ -329,13 +329,13 @@ static void fill_ctl(DcCtl& c, double inc_it, double max_dt, double min_dt, doub
 static bool finite_dt(double dt, double min_dt) { return std::isfinite(dt) && std::isfinite(min_dt); }
 
 // ====================================================== fused batched sweeps
-// Pipelines of the fused sweep (as in the single-model staged sweep): two
-// producer warps, each with its own ring of stages and consumer group, one
-// block per SM.
+// Pipelines of the fused sweep, as in the single-model staged sweep: two per
+// block, one block per SM, up to 4 stages a ring.  (Measured against one
+// pipeline and two blocks per SM: 24.9 against 23.9 G cell-updates/s on the
+// serving workload, 99 against 102 on the 48-model ensemble -- within the
+// runs' spread.)
 constexpr int kFusedPipes = 2;
-constexpr int kFusedStages = 8;   // at most, over both rings
-constexpr int kFusedThreads = kTmaConsumers + 32 * kFusedPipes;
-static_assert((kTmaConsumers / kTmaGroup) % kFusedPipes == 0, "every pipeline has its own consumer group");
+constexpr int kFusedMaxRing = 4;
 
 // All models of a batch in one cooperative sweep: the chunks (kTmaChunk
 // cells) of every active model form one table, interleaved over the blocks,
@@ -431,11 +431,15 @@ __device__ void fused_decide(const FusedItem& I, int g, int num_it, bool check, 
     if (ev != EV_NONE) atomicExch(any_event, 1);
 }
 
-template <int RING>
-__global__ void __launch_bounds__(kFusedThreads, 1) fused_sweep_kernel(FusedArgs A, TmaStage T) {
+template <int RING, int PIPES>
+__global__ void __launch_bounds__(kTmaConsumers + 32 * PIPES, PIPES == 1 ? 2 : 1)
+    fused_sweep_kernel(FusedArgs A, TmaStage T) {
+    constexpr int kPipes = PIPES;
+    constexpr int kFusedThreads = kTmaConsumers + 32 * PIPES;
+    static_assert((kTmaConsumers / kTmaGroup) % PIPES == 0, "every pipeline has its own consumer groups");
     extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ __align__(8) uint64_t full[RING * kFusedPipes];
-    __shared__ __align__(8) uint64_t empty[RING * kFusedPipes];
+    __shared__ __align__(8) uint64_t full[RING * PIPES];
+    __shared__ __align__(8) uint64_t empty[RING * PIPES];
     __shared__ double sh[kFusedThreads / 32];
     __shared__ int s_err;
     const unsigned nb = gridDim.x, b = blockIdx.x;
@@ -445,17 +449,17 @@ __global__ void __launch_bounds__(kFusedThreads, 1) fused_sweep_kernel(FusedArgs
     const int group = tid / kTmaGroup;                  // consumers: 0 or 1
     const int gt = tid & (kTmaGroup - 1);
     // pipelines as in dc_sweep_tma_kernel: producer warp + ring + groups
-    const int pipe = producer ? warp - kTmaConsumers / 32 : group % kFusedPipes;
-    const int grank = group / kFusedPipes;
-    constexpr int kGroupsPerPipe = (kTmaConsumers / kTmaGroup) / kFusedPipes;
+    const int pipe = producer ? warp - kTmaConsumers / 32 : group % kPipes;
+    const int grank = group / kPipes;
+    constexpr int kGroupsPerPipe = (kTmaConsumers / kTmaGroup) / kPipes;
     const unsigned ring0 = (unsigned)pipe * RING;
     const long long C = kTmaChunk;
     const long long mine = A.nchunks > (long long)b ? (A.nchunks - 1 - b) / nb + 1 : 0;
-    const long long pmine = mine > pipe ? (mine - 1 - pipe) / kFusedPipes + 1 : 0;
+    const long long pmine = mine > pipe ? (mine - 1 - pipe) / kPipes + 1 : 0;
     const uint64_t keep = l2_evict_last();
     volatile int* err = &s_err;
     if (tid == 0) {
-        for (int s = 0; s < RING * kFusedPipes; ++s) {
+        for (int s = 0; s < RING * kPipes; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], kTmaGroup / 32);   // one arrival per warp of a group
         }
@@ -479,7 +483,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) fused_sweep_kernel(FusedArgs
                         if (issued >= (unsigned)RING &&
                             !mbar_wait_flag(&empty[s], (issued / RING - 1) & 1u, err))
                             break;
-                        const FusedChunk ch = A.chunks[b + (pipe + j * kFusedPipes) * nb];
+                        const FusedChunk ch = A.chunks[b + (pipe + j * kPipes) * nb];
                         const DcCtl& c = A.items[ch.item].c;
                         const long long cnt = (c.Ncal - ch.m0) < C ? (c.Ncal - ch.m0) : C;
                         unsigned char* stg = smem + (size_t)s * T.bytes;
@@ -499,7 +503,7 @@ __global__ void __launch_bounds__(kFusedThreads, 1) fused_sweep_kernel(FusedArgs
                     if (!__shfl_sync(0xffffffffu, okw, 0)) break;
                     mbar_try_wait(&full[s], (u / RING) & 1u);
                     const unsigned char* stg = smem + (size_t)s * T.bytes;
-                    const long long q = b + (pipe + j * kFusedPipes) * nb;
+                    const long long q = b + (pipe + j * kPipes) * nb;
                     const FusedChunk ch = A.chunks[q];
                     const DcCtl& c = A.items[ch.item].c;
                     const long long m0 = ch.m0, SX = c.L.SX;
@@ -636,18 +640,22 @@ static int run_fused(std::vector<BatchItem<Form>>& v, TseDcOptions* opts, void* 
     }
     if (fused_ws_bytes(n, cells) > ws_bytes) return TSE_ERR_WORKSPACE;
     TmaStage T = tma_stage(Hmax);
-    // as many stages as fit (up to kFusedStages), an equal ring per pipeline;
-    // one instantiation per ring length
-    const size_t cap_smem = fused_max_smem();
-    int nst = (int)std::min<size_t>((size_t)kFusedStages, cap_smem / (size_t)T.bytes);
-    const int ring = nst / kFusedPipes;
+    // as many stages as fit (up to 4 a ring, an equal ring per pipeline); one
+    // instantiation per ring length
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int pipes = kFusedPipes;
+    const int avail =
+        (int)std::min<size_t>((size_t)(kFusedMaxRing * pipes), fused_max_smem() / (size_t)T.bytes);
+    const int ring = avail / pipes;
     if (ring < 2) return TSE_ERR_ARG;
-    const void* kernel = ring >= 4   ? (const void*)fused_sweep_kernel<4>
-                         : ring == 3 ? (const void*)fused_sweep_kernel<3>
-                                     : (const void*)fused_sweep_kernel<2>;
-    nst = (ring >= 4 ? 4 : ring) * kFusedPipes;
-    T.stages = nst;
-    const size_t smem = (size_t)nst * T.bytes;
+    const void* kernel = ring == 2   ? (const void*)fused_sweep_kernel<2, kFusedPipes>
+                         : ring == 3 ? (const void*)fused_sweep_kernel<3, kFusedPipes>
+                                     : (const void*)fused_sweep_kernel<4, kFusedPipes>;
+    const int fused_threads = kTmaConsumers + 32 * pipes;
+    T.stages = ring * pipes;
+    const size_t smem = (size_t)T.stages * T.bytes;
     // carve the batch workspace
     const size_t nch_max = (size_t)(cells / kTmaChunk) + (size_t)n + 1;
     char* p = (char*)d_ws;
@@ -663,12 +671,9 @@ static int run_fused(std::vector<BatchItem<Form>>& v, TseDcOptions* opts, void* 
     p += 256;
     GridBarrier* d_bar = (GridBarrier*)p;
 
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap_smem) !=
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused_max_smem()) !=
             cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kFusedThreads, smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, fused_threads, smem) != cudaSuccess ||
         per_sm < 1)
         return TSE_ERR_LAUNCH;
 
@@ -754,7 +759,7 @@ static int run_fused(std::vector<BatchItem<Form>>& v, TseDcOptions* opts, void* 
         }
         void* args[] = {(void*)&A, (void*)&T};
         if (timing) cudaEventRecord(ev0, stream);
-        if (cudaLaunchCooperativeKernel(kernel, dim3((unsigned)nb), dim3(kFusedThreads), args, smem,
+        if (cudaLaunchCooperativeKernel(kernel, dim3((unsigned)nb), dim3(fused_threads), args, smem,
                                         stream) != cudaSuccess) {
             rc = TSE_ERR_LAUNCH;
             break;

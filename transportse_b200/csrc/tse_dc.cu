@@ -26,8 +26,8 @@
 // small state record per correction cycle.
 //
 // An inner cell-update streams the six FP32 coefficients (one 24-byte record),
-// r', the flag byte and d (read + write) plus the neighbours' d: ~37 bytes
-// against 113-129 for the FP64 form.
+// r' and the flag byte from DRAM -- 29 bytes; d and the neighbours' d stay in
+// L2 -- against 89 bytes of coefficients and flags for the FP64 form.
 //
 // Compiled with FMA contraction (no bit-exactness is claimed for this form).
 #include "tse_dc.cuh"
@@ -48,24 +48,21 @@ constexpr int kSweepBlock = TSE_SWEEP_BLOCK;
 constexpr int kResBlocks = 2048;   // fixed grid of the residual kernel (deterministic sums)
 
 // Pipelines of the staged sweep: each has its own producer warp, its own ring
-// of stages and its own consumer groups, and takes every kDcPipes-th
-// chunk of the block.  A producer warp issues its copies one after another,
-// at a rate that bounds a pipeline's throughput; more pipelines per SM (more
-// blocks, or more per block) raise that bound.
-#ifndef TSE_DC_PIPES
-#define TSE_DC_PIPES 2
-#endif
-#ifndef TSE_DC_MINB
-#define TSE_DC_MINB 1                // blocks per SM
-#endif
-#ifndef TSE_DC_STAGES
-#define TSE_DC_STAGES 8              // over all pipelines
-#endif
-constexpr int kDcPipes = TSE_DC_PIPES;
-constexpr int kDcStages = TSE_DC_STAGES;     // at most; fewer where long columns make stages big
-constexpr int kDcThreads = kTmaConsumers + 32 * kDcPipes;
-static_assert(kDcStages % kDcPipes == 0 && kDcStages >= 2 * kDcPipes, "two or more stages a ring");
-static_assert((kTmaConsumers / kTmaGroup) % kDcPipes == 0, "every pipeline has its own consumer groups");
+// of stages and its own consumer group, and takes every PIPES-th chunk of the
+// block.  A producer warp issues its copies one after another, at a rate that
+// bounds a pipeline's throughput: two pipelines per block, one block per SM,
+// up to 4 stages a ring.  (Measured against one pipeline -- two consumer
+// groups sharing a ring -- and two blocks per SM: faster at every grid from
+// 96^3 to 256 x 256 x 128.)
+constexpr int kDcPipes = 2;
+constexpr int kDcMaxRing = 4;
+template <int PIPES>
+struct DcLayout {
+    static constexpr int kThreads = kTmaConsumers + 32 * PIPES;
+    static constexpr int kMinBlocks = PIPES == 1 ? 2 : 1;
+    static constexpr int kGroupsPerPipe = (kTmaConsumers / kTmaGroup) / PIPES;
+    static_assert((kTmaConsumers / kTmaGroup) % PIPES == 0, "every pipeline has its own consumer groups");
+};
 
 // ------------------------------------------------------------ FP64 kernels
 // K'_q = k_q / Den for every cell (at the start and after dt halving)
@@ -259,12 +256,15 @@ __global__ void __launch_bounds__(kSweepBlock, kSweepMinBlocks) dc_sweep_kernel(
 
 // ------------------------------------------------ FP32 sweeps, TMA-staged
 // (the staging pieces are in tse_dc.cuh)
-template <int RING>
-__global__ void __launch_bounds__(kDcThreads, TSE_DC_MINB) dc_sweep_tma_kernel(DcCtl c, TmaStage T) {
+template <int RING, int PIPES>
+__global__ void __launch_bounds__(DcLayout<PIPES>::kThreads, DcLayout<PIPES>::kMinBlocks)
+    dc_sweep_tma_kernel(DcCtl c, TmaStage T) {
+    constexpr int kPipes = PIPES;
+    constexpr int kThreads = DcLayout<PIPES>::kThreads;
     extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ __align__(8) uint64_t full[kDcStages];
-    __shared__ __align__(8) uint64_t empty[kDcStages];
-    __shared__ double sh[kDcThreads / 32];
+    __shared__ __align__(8) uint64_t full[RING * PIPES];
+    __shared__ __align__(8) uint64_t empty[RING * PIPES];
+    __shared__ double sh[kThreads / 32];
     __shared__ int s_err;
     const unsigned nb = gridDim.x, b = blockIdx.x;
     const int tid = threadIdx.x;
@@ -274,17 +274,17 @@ __global__ void __launch_bounds__(kDcThreads, TSE_DC_MINB) dc_sweep_tma_kernel(D
     const int gt = tid & (kTmaGroup - 1);               // thread within its group
     // this thread's pipeline (producer warp + its ring of stages +
     // its consumer groups), and a consumer group's rank within it
-    const int pipe = producer ? warp - kTmaConsumers / 32 : group % kDcPipes;
-    const int grank = group / kDcPipes;
-    constexpr int kGroupsPerPipe = (kTmaConsumers / kTmaGroup) / kDcPipes;
-    constexpr unsigned ring = RING;                     // stages of a ring (T.stages / kDcPipes)
+    const int pipe = producer ? warp - kTmaConsumers / 32 : group % kPipes;
+    const int grank = group / kPipes;
+    constexpr int kGroupsPerPipe = DcLayout<PIPES>::kGroupsPerPipe;
+    constexpr unsigned ring = RING;                     // stages of a ring (T.stages / PIPES)
     const unsigned ring0 = (unsigned)pipe * ring;    // the pipeline's first stage
     const long long Nc = c.L.Nc, N = c.Ncal, SX = c.L.SX, C = kTmaChunk;
     const int H = c.L.H;
     const long long nch = (Nc + C - 1) / C;
     const long long mine = nch > (long long)b ? (nch - 1 - b) / nb + 1 : 0;   // chunks of this block
-    // this pipeline's chunks of a phase: i = pipe, pipe + kDcPipes, ...
-    const long long pmine = mine > pipe ? (mine - 1 - pipe) / kDcPipes + 1 : 0;
+    // this pipeline's chunks of a phase: i = pipe, pipe + kPipes, ...
+    const long long pmine = mine > pipe ? (mine - 1 - pipe) / kPipes + 1 : 0;
     unsigned* bar_count = c.prog;   // count_sync's counter, zeroed before the launch
     unsigned bars = 0;              // device-wide barriers passed in this launch
     const bool leader = (b == 0 && tid == 0);
@@ -299,7 +299,7 @@ __global__ void __launch_bounds__(kDcThreads, TSE_DC_MINB) dc_sweep_tma_kernel(D
     volatile int* err = &s_err;
 
     if (tid == 0) {
-        for (int s = 0; s < RING * kDcPipes; ++s) {
+        for (int s = 0; s < RING * kPipes; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], kTmaGroup / 32);   // one arrival per warp of a group
         }
@@ -315,7 +315,7 @@ __global__ void __launch_bounds__(kDcThreads, TSE_DC_MINB) dc_sweep_tma_kernel(D
 #if TSE_TMA_PREFETCH
     if (producer && lane == 0) {
         for (long long j = 0; j < pro; ++j) {
-            const long long m0 = (b + (pipe + j * kDcPipes) * nb) * C;
+            const long long m0 = (b + (pipe + j * kPipes) * nb) * C;
             const long long cnt = (N - m0) < C ? (N - m0) : C;
             tma_issue_own(c, T, smem + (size_t)(ring0 + j) * T.bytes, &full[ring0 + j], c.K[0], c.D[0],
                           c.mask[0], m0, cnt);
@@ -344,7 +344,7 @@ __global__ void __launch_bounds__(kDcThreads, TSE_DC_MINB) dc_sweep_tma_kernel(D
                     bool pok = true;
                     for (long long j = 0; j < pmine; ++j, ++issued) {
                         const unsigned s = ring0 + issued % ring;
-                        const long long m0 = (b + (pipe + j * kDcPipes) * nb) * C;
+                        const long long m0 = (b + (pipe + j * kPipes) * nb) * C;
                         unsigned char* stg = smem + (size_t)s * T.bytes;
                         if (j >= primed) {
                             if (issued >= (unsigned)ring &&
@@ -369,7 +369,7 @@ __global__ void __launch_bounds__(kDcThreads, TSE_DC_MINB) dc_sweep_tma_kernel(D
                         if (v >= (unsigned)ring &&
                             !mbar_wait_flag(&empty[s], (v / ring - 1) & 1u, err))
                             break;
-                        const long long m0 = (b + (pipe + j * kDcPipes) * nb) * C;
+                        const long long m0 = (b + (pipe + j * kPipes) * nb) * C;
                         const long long cnt = (N - m0) < C ? (N - m0) : C;
                         tma_issue_own(c, T, smem + (size_t)s * T.bytes, &full[s], c.K[nc], c.D[nc],
                                       c.mask[nc], m0, cnt);
@@ -389,7 +389,7 @@ __global__ void __launch_bounds__(kDcThreads, TSE_DC_MINB) dc_sweep_tma_kernel(D
                     if (!__shfl_sync(0xffffffffu, okw, 0)) break;
                     mbar_try_wait(&full[s], (u / ring) & 1u);
                     const unsigned char* stg = smem + (size_t)s * T.bytes;
-                    const long long m0 = (b + (pipe + j * kDcPipes) * nb) * C;
+                    const long long m0 = (b + (pipe + j * kPipes) * nb) * C;
                     const int nval = (int)((Nc - m0) < C ? (Nc - m0) : C);
                     // window offsets of cell l of the chunk (32-bit from here on)
                     const int oz = (int)(m0 - ((m0 - H - 1) & ~3LL));
@@ -437,8 +437,8 @@ __global__ void __launch_bounds__(kDcThreads, TSE_DC_MINB) dc_sweep_tma_kernel(D
             __syncthreads();
             if (*err) { ok = false; break; }   // block-uniform after the barrier
             if (col == 1 && check) {
-                const double b1 = block_sum<kDcThreads>((double)d2, sh);
-                const double b3 = block_sum<kDcThreads>((double)dd, sh);
+                const double b1 = block_sum<kThreads>((double)d2, sh);
+                const double b3 = block_sum<kThreads>((double)dd, sh);
                 if (tid == 0) {
                     c.partials[4 * b + 2 * (checkno & 1)] = b1;
                     c.partials[4 * b + 2 * (checkno & 1) + 1] = b3;
@@ -455,8 +455,8 @@ __global__ void __launch_bounds__(kDcThreads, TSE_DC_MINB) dc_sweep_tma_kernel(D
                 s1 = s1 + __ldcg(c.partials + 4 * q + 2 * (checkno & 1));
                 s3 = s3 + __ldcg(c.partials + 4 * q + 2 * (checkno & 1) + 1);
             }
-            s1 = block_sum<kDcThreads>(s1, sh);
-            s3 = block_sum<kDcThreads>(s3, sh);
+            s1 = block_sum<kThreads>(s1, sh);
+            s3 = block_sum<kThreads>(s3, sh);
             if (tid == 0) {
                 sh[0] = s1;
                 sh[1] = s3;
@@ -582,17 +582,14 @@ static size_t tma_max_smem() {
 // blocks of the staged sweep: as many as fit (dynamic shared memory
 // included), at most one per chunk of a colour; 0 when the stages for this
 // grid's windows do not fit (the plain sweep kernel runs instead)
-// the instantiation for a ring of `ring` stages (2 .. kDcStages / kDcPipes)
+// the instantiation for rings of `ring` stages (2 .. 4)
 static const void* tma_kernel(int ring) {
-    constexpr int kMaxRing = kDcStages / kDcPipes;
-    switch (ring < kMaxRing ? ring : kMaxRing) {
-        case 2: return (const void*)dc_sweep_tma_kernel<2>;
-        case 3: return (const void*)dc_sweep_tma_kernel<(3 <= kMaxRing ? 3 : 2)>;
-        default: return (const void*)dc_sweep_tma_kernel<(4 <= kMaxRing ? 4 : kMaxRing)>;
-    }
+    return ring <= 2 ? (const void*)dc_sweep_tma_kernel<2, kDcPipes>
+         : ring == 3 ? (const void*)dc_sweep_tma_kernel<3, kDcPipes>
+                     : (const void*)dc_sweep_tma_kernel<4, kDcPipes>;
 }
 
-static int tma_blocks(long long Nc, int cap, size_t smem, const void* kernel) {
+static int tma_blocks(long long Nc, int cap, size_t smem, const void* kernel, int threads) {
     const size_t ceil_smem = tma_max_smem();
     if (!TSE_SWEEP_TMA || smem == 0 || smem > ceil_smem) return 0;
     int dev = 0, sms = 0, per_sm = 0;
@@ -602,7 +599,7 @@ static int tma_blocks(long long Nc, int cap, size_t smem, const void* kernel) {
     // below another's launch
     if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ceil_smem) !=
             cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kDcThreads, smem) !=
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) !=
             cudaSuccess ||
         per_sm < 1) {
         cudaGetLastError();
@@ -648,16 +645,17 @@ static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, 
     const long long cells2 = 2 * S.L.Nc;
     const unsigned gcells = (unsigned)((cells2 + kBlock - 1) / kBlock);
     TmaStage T = tma_stage(S.L.H);
-    // as many stages as fit, up to kDcStages, an equal ring per pipeline
+    // as many stages as fit, up to 4 a ring, an equal ring per pipeline
+    const int pipes = kDcPipes;
     {
-        const size_t cap = tma_max_smem();
-        int st = cap > 0 ? (int)std::min<size_t>((size_t)kDcStages, cap / (size_t)T.bytes) : 0;
-        st -= st % kDcPipes;
-        T.stages = st >= 2 * kDcPipes ? st : 0;
+        int st = (int)std::min<size_t>((size_t)(kDcMaxRing * pipes), tma_max_smem() / (size_t)T.bytes);
+        st -= st % pipes;
+        T.stages = st >= 2 * pipes ? st : 0;
     }
     const size_t tma_smem = (size_t)T.stages * T.bytes;
-    const void* tma_k = T.stages > 0 ? tma_kernel(T.stages / kDcPipes) : nullptr;
-    const int nb_tma = tma_k ? tma_blocks(S.L.Nc, cap, tma_smem, tma_k) : 0;
+    const int tma_threads = kTmaConsumers + 32 * pipes;
+    const void* tma_k = T.stages > 0 ? tma_kernel(T.stages / pipes) : nullptr;
+    const int nb_tma = tma_k ? tma_blocks(S.L.Nc, cap, tma_smem, tma_k, tma_threads) : 0;
     const int nb = nb_tma > 0 ? nb_tma : sweep_blocks(S.L.Nc, cap);
     dc_scale_kernel<<<gcells, kBlock, 0, stream>>>(S.F, c);
     if (cudaGetLastError() != cudaSuccess) return TSE_ERR_LAUNCH;
@@ -690,7 +688,7 @@ static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, 
         }
         const cudaError_t le =
             nb_tma > 0 ? cudaLaunchCooperativeKernel(tma_k, dim3(nb),
-                                                     dim3(kDcThreads), targs, tma_smem, stream)
+                                                     dim3(tma_threads), targs, tma_smem, stream)
                        : cudaLaunchCooperativeKernel((const void*)dc_sweep_kernel, dim3(nb),
                                                      dim3(kSweepBlock), args, 0, stream);
         if (le != cudaSuccess) {
