@@ -69,7 +69,9 @@ def _pressure_case(shape, seed):
 SHAPES = [(33, 17, 21), (1, 1, 40), (16, 16, 16), (9, 1, 31), (40, 30, 24), (5, 7, 3)]
 # column heights far apart in one batch: the stage layout is sized for the
 # tallest column, each model's windows for its own
-MIXED_H = [(2, 2, 600), (60, 40, 2), (12, 9, 7)]
+# column heights from 2 to 1600: the fused sweep sizes its stages for the
+# tallest, whose stages leave room for rings of 3
+MIXED_H = [(2, 2, 600), (60, 40, 2), (12, 9, 7), (1, 2, 1600)]
 
 
 @pytest.mark.parametrize("cluster", [0, 1, 4, 16])

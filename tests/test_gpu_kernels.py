@@ -151,7 +151,10 @@ def test_mass_totals_vs_numpy(cuda_device):
     assert len(sim.mass_log) == 2
 
 
-@pytest.mark.parametrize("shape", [(64, 48, 40), (37, 23, 51), (96, 96, 64)])
+# (3, 2, 1000): stages big enough that the rings hold 2 stages; (1, 2, 3000):
+# the pressure solve's stages fit no ring (the plain kernel runs in both modes),
+# the species solve's rings hold 2
+@pytest.mark.parametrize("shape", [(64, 48, 40), (37, 23, 51), (96, 96, 64), (3, 2, 1000), (1, 2, 3000)])
 def test_staged_and_plain_exact_solves_agree(shape, cuda_device):
     """The staged FP64 sweep (bulk copies into shared-memory stages) and the
     plain-load sweep compute every cell with the same operations: over whole

@@ -232,7 +232,8 @@ def test_staged_sweep_copies_stay_aligned_and_in_bounds():
     import random
     rng = random.Random(5)
     shapes = [(1, 1, 1), (1, 1, 2), (2, 1, 1), (3, 3, 3), (1, 1, 40), (9, 1, 31), (5, 7, 3),
-              (60, 1, 30), (33, 17, 21), (2, 2, 600), (60, 40, 2), (64, 64, 32), (128, 96, 77)]
+              (60, 1, 30), (33, 17, 21), (2, 2, 600), (60, 40, 2), (64, 64, 32), (128, 96, 77),
+              (1, 2, 1600), (1, 2, 4000)]
     shapes += [(rng.randint(1, 40), rng.randint(1, 40), rng.randint(1, 300)) for _ in range(60)]
     # single model: the stage fits its own H; fused batch: the tallest column's
     Hmax = max((nz + (nz & 1)) // 2 for _, _, nz in shapes)
@@ -330,7 +331,8 @@ def test_exact_staged_copies_stay_aligned_and_in_bounds():
     import random
     rng = random.Random(11)
     shapes = [(1, 1, 1), (1, 1, 2), (2, 1, 1), (3, 3, 3), (1, 1, 40), (9, 1, 31), (5, 7, 3),
-              (60, 1, 30), (33, 17, 21), (2, 2, 600), (60, 40, 2), (24, 24, 20), (7, 3, 257)]
+              (60, 1, 30), (33, 17, 21), (2, 2, 600), (60, 40, 2), (24, 24, 20), (7, 3, 257),
+              (3, 2, 1000), (1, 2, 3000)]
     shapes += [(rng.randint(1, 24), rng.randint(1, 24), rng.randint(1, 120)) for _ in range(40)]
     for nx, ny, nz in shapes:
         for nst, count, sol in ((9, 17, 16), (11, 17, 16), (13, 17, 16),   # pressure
