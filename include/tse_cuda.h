@@ -355,6 +355,22 @@ int32_t tse_selftest_bounded_waits(int32_t *d_result, double timeout_s, void *d_
  * mode, or TSE_ERR_ARG for a mode other than 0 or 1. */
 int32_t tse_set_exact_sweep(int32_t mode);
 
+/* Loop of the fused batched form (tse_compute_*_dc_batch with max_blocks <= 0;
+ * no counterpart in the reference): 1 (default) = device-driven, the whole
+ * solve of the batch one CUDA graph launch (a conditional WHILE node whose body
+ * plans the launch, sweeps, handles each model's events and forms the
+ * residuals on the device; the call reads one small record at the end), 0 = a
+ * host loop that reads the models' states after every sweep launch and queues
+ * their next steps.  Both give the same results bit for bit; the device-driven
+ * loop falls back to the host loop where a graph cannot be built (the legacy
+ * default stream).  With opts->timing the device-driven loop reports the whole
+ * loop's event time in sweep_ms.  Applies to calls made after it; returns the
+ * previous mode, or TSE_ERR_ARG for a mode other than 0 or 1. */
+int32_t tse_set_batch_loop(int32_t mode);
+
+/* Batched solves run so far by the device-driven loop and by the host loop. */
+int32_t tse_batch_loop_stats(int64_t *graph_solves, int64_t *host_solves);
+
 /* Library version string. */
 const char *tse_version(void);
 

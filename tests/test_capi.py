@@ -121,3 +121,20 @@ def test_exact_sweep_mode_switch_without_gpu():
         assert L.tse_set_exact_sweep(2) == -1 and L.tse_set_exact_sweep(-1) == -1
     finally:
         L.tse_set_exact_sweep(prev)
+
+
+def test_batch_loop_switch_and_stats_without_gpu():
+    """The batched form's loop selector takes 0 or 1 and returns the previous
+    mode; the loop statistics read without a device call."""
+    L = N.lib()
+    prev = L.tse_set_batch_loop(0)
+    try:
+        assert prev in (0, 1)
+        assert L.tse_set_batch_loop(1) == 0
+        assert L.tse_set_batch_loop(3) == -1
+    finally:
+        L.tse_set_batch_loop(prev)
+    g, h = ct.c_int64(-1), ct.c_int64(-1)
+    assert L.tse_batch_loop_stats(ct.byref(g), ct.byref(h)) == 0
+    assert g.value >= 0 and h.value >= 0
+    assert L.tse_batch_loop_stats(None, ct.byref(h)) == -1

@@ -105,6 +105,48 @@ def test_batched_pressure_equals_single_solves(cluster, cuda_device):
         assert rel_err(g[2], ro[2]) <= TOL, SHAPES[i]
 
 
+@pytest.mark.parametrize("kw", [
+    dict(SOR=1.7, max_it=20000, inc_it=1.25, max_dt=1e5, min_dt=1e-8, P_conv=1e-10),
+    dict(SOR=1.7, max_it=25, inc_it=1.25, max_dt=1e5, min_dt=400.0, P_conv=1e-12)])
+def test_device_loop_equals_host_loop(kw, cuda_device):
+    """The fused form's device-driven loop (one CUDA graph: a conditional WHILE
+    node around plan, sweep, events and residual kernels) and its host loop
+    take the same steps: every model's pressure, t, dt, convergence flag and
+    iteration count agree bit for bit -- through cycle ends and refreshes
+    (first case) and through dt halvings down to min_dt (second)."""
+    import ctypes as ct
+    from transportse_b200 import _native
+    lib = _native.lib()
+    cases_ = [_pressure_case(s, 7 + i) for i, s in enumerate(SHAPES)]
+
+    def member(i):
+        cfg, P, rest = cases_[i]
+
+        def fn(gate):
+            m = model_for(cfg, cuda_device, "fp32dc")
+            m.batch_gate = gate
+            return NumpyKernels(m).compute_P(P.copy(), *rest, **kw)
+        return fn
+
+    out, used = {}, {}
+    prev = lib.tse_set_batch_loop(1)
+    try:
+        for mode in (1, 0):
+            lib.tse_set_batch_loop(mode)
+            g0, h0 = ct.c_int64(), ct.c_int64()
+            lib.tse_batch_loop_stats(ct.byref(g0), ct.byref(h0))
+            out[mode], _ = _run_members([member(i) for i in range(len(SHAPES))], cuda_device)
+            g1, h1 = ct.c_int64(), ct.c_int64()
+            lib.tse_batch_loop_stats(ct.byref(g1), ct.byref(h1))
+            used[mode] = (g1.value - g0.value, h1.value - h0.value)
+    finally:
+        lib.tse_set_batch_loop(prev)
+    assert used[1] == (1, 0) and used[0] == (0, 1), used
+    for i, (a, b) in enumerate(zip(out[1], out[0])):
+        assert (a[0], a[1], a[4], a[5]) == (b[0], b[1], b[4], b[5]), SHAPES[i]
+        assert numpy.array_equal(a[2], b[2]), SHAPES[i]
+
+
 def test_batched_halving_and_stop_follow_the_reference(cuda_device):
     # unreachable tolerance: every solve halves dt max_it by max_it until it
     # reaches min_dt, then stops unconverged (tse.py:724-740)

@@ -125,6 +125,8 @@ SIGNATURES = {
                              _P]),
     "tse_selftest_bounded_waits": (_I, [_P, _D, _P, _S, _P]),
     "tse_set_exact_sweep": (_I, [_I]),
+    "tse_set_batch_loop": (_I, [_I]),
+    "tse_batch_loop_stats": (_I, [ct.POINTER(ct.c_int64), ct.POINTER(ct.c_int64)]),
     "tse_version": (ct.c_char_p, []),
 }
 

@@ -22,6 +22,7 @@
 #include <cmath>
 #include <vector>
 #include <algorithm>
+#include <atomic>
 #include <cooperative_groups.h>
 
 #include "tse_dc.cuh"
@@ -432,8 +433,7 @@ __device__ void fused_decide(const FusedItem& I, int g, int num_it, bool check, 
 }
 
 template <int RING, int PIPES>
-__global__ void __launch_bounds__(kTmaConsumers + 32 * PIPES, PIPES == 1 ? 2 : 1)
-    fused_sweep_kernel(FusedArgs A, TmaStage T) {
+__device__ __forceinline__ void fused_sweep_body(const FusedArgs& A, const TmaStage& T) {
     constexpr int kPipes = PIPES;
     constexpr int kFusedThreads = kTmaConsumers + 32 * PIPES;
     static_assert((kTmaConsumers / kTmaGroup) % PIPES == 0, "every pipeline has its own consumer groups");
@@ -603,6 +603,21 @@ __global__ void __launch_bounds__(kTmaConsumers + 32 * PIPES, PIPES == 1 ? 2 : 1
         for (int it = 0; it < A.nitems; ++it) A.items[it].c.st->event = EV_ERROR;
 }
 
+template <int RING, int PIPES>
+__global__ void __launch_bounds__(kTmaConsumers + 32 * PIPES, PIPES == 1 ? 2 : 1)
+    fused_sweep_kernel(FusedArgs A, TmaStage T) {
+    fused_sweep_body<RING, PIPES>(A, T);
+}
+
+// the same with its arguments in device memory, written by the plan kernel
+// of the device-driven loop
+template <int RING, int PIPES>
+__global__ void __launch_bounds__(kTmaConsumers + 32 * PIPES, PIPES == 1 ? 2 : 1)
+    fused_sweep_dev_kernel(const FusedArgs* Ad, TmaStage T) {
+    const FusedArgs A = *Ad;
+    fused_sweep_body<RING, PIPES>(A, T);
+}
+
 __global__ void fused_gather_kernel(const FusedItem* items, int n, DcState* out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] = *items[i].c.st;
@@ -620,12 +635,15 @@ static size_t fused_max_smem() {
     return optin > 2048 ? (size_t)optin - 2048 : 0;
 }
 
+// bytes the device-driven loop adds to the batch workspace (defined with it)
+static size_t fused_loop_bytes(int n);
+
 // bytes of the fused form's batch workspace for n models of `cells` cells in all
 static size_t fused_ws_bytes(int n, long long cells) {
     const size_t nch = (size_t)(cells / kTmaChunk) + (size_t)n + 1;
     return align256(sizeof(FusedItem) * n) + align256(sizeof(FusedChunk) * nch) +
            align256(sizeof(double2) * 8 * nch) + align256(sizeof(DcState) * n) + 256 +
-           align256(sizeof(GridBarrier)) + 256;
+           align256(sizeof(GridBarrier)) + 256 + fused_loop_bytes(n);
 }
 
 template <class Form>
@@ -833,9 +851,518 @@ static int run_fused(std::vector<BatchItem<Form>>& v, TseDcOptions* opts, void* 
     return rc;
 }
 
+// ------------------------------------------------ device-driven fused solves
+// run_fused's host loop reads every model's state after each sweep launch and
+// queues the models' next steps.  Here the same loop runs on the device, as a
+// CUDA graph holding one conditional WHILE node whose body is
+//   plan -> chunk table -> fused sweep -> events -> x += d / dt halving
+//        -> residual -> x^2
+// so the host launches the graph once per batch solve and reads one small
+// record when it ends.  Each step computes what run_fused's host code and
+// its per-model kernels compute, in the same order and blocking -- a model's
+// residual runs as the same res_blocks(Nc) blocks of residual_block_cells, its
+// x^2 is summed as dc_x2_kernel sums it -- so the results are run_fused's bit
+// for bit.  The body runs at most kGraphMaxRuns times per graph launch (the
+// host relaunches the graph while models remain), so no launch can loop on
+// the device without end.
+
+struct FusedCtl {
+    int n;                   // models of the batch
+    int nactive;             // models still solving, after the last events pass
+    int num_it;              // the models' global iteration count
+    int failed;              // a sweep reported EV_ERROR
+    int runs;                // loop-body runs in the current graph launch
+    int launches;            // sweep launches over the whole solve
+    long long iterations;    // global iterations over the whole solve
+    long long resid_total;   // residual blocks of the current body run, all models
+};
+
+// one model of the device-driven loop
+struct FusedModel {
+    DcCtl c;
+    long long nchunks;       // ceil(Nc / kTmaChunk)
+    int active;              // 1 while solving
+    int inner;               // iterations since the model's last residual
+};
+
+enum : int { ACT_APPLY = 1, ACT_HALVE = 2, ACT_RESID = 4 };
+constexpr int kGraphMaxRuns = 4096;
+constexpr int kPlanThreads = 1024;
+
+// inclusive block-wide prefix sum; *total gets the block's sum
+template <typename V>
+__device__ V block_inclusive_scan(V v, V* sh, V* total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const V u = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += u;
+    }
+    if (lane == 31) sh[w] = v;
+    __syncthreads();
+    if (w == 0) {
+        V x = lane < nw ? sh[lane] : V(0);
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const V u = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += u;
+        }
+        sh[lane] = x;
+    }
+    __syncthreads();
+    if (w > 0) v += sh[w - 1];
+    *total = sh[nw - 1];
+    __syncthreads();
+    return v;
+}
+
+// the active models in index order, their iteration limit for the launch
+// (run_fused's g_max), their chunk ranges and the sweep's arguments
+__global__ void __launch_bounds__(kPlanThreads) fused_plan_kernel(const FusedCtl* ctl, const FusedModel* models,
+                                                                  FusedItem* items, int* idx, FusedArgs* args,
+                                                                  FusedChunk* chunks, double2* cpart,
+                                                                  int* any_event, GridBarrier* bar) {
+    __shared__ long long sh_ll[32];
+    __shared__ int sh_i[32];
+    __shared__ int s_gmax, s_base_k;
+    __shared__ long long s_base_ch;
+    const int n = ctl->n;
+    if (threadIdx.x == 0) {
+        s_gmax = 1 << 30;
+        s_base_k = 0;
+        s_base_ch = 0;
+    }
+    __syncthreads();
+    for (int base = 0; base < n; base += kPlanThreads) {
+        const int i = base + threadIdx.x;
+        int a = 0;
+        long long nc = 0;
+        if (i < n && models[i].active) {
+            const FusedModel& M = models[i];
+            const DcState* st = M.c.st;
+            a = 1;
+            nc = M.nchunks;
+            int lim = M.c.cycle - M.inner;
+            const int h = M.c.max_it - st->num_sub_it;
+            lim = h < lim ? h : lim;
+            if (st->dt <= M.c.min_dt) lim = 1;
+            atomicMin(&s_gmax, lim);
+        }
+        int tot_a;
+        long long tot_c;
+        const int pa = block_inclusive_scan<int>(a, sh_i, &tot_a);
+        const long long pc = block_inclusive_scan<long long>(nc, sh_ll, &tot_c);
+        if (a) {
+            const int k = s_base_k + pa - 1;
+            FusedItem I;
+            I.c = models[i].c;
+            I.cfirst = s_base_ch + pc - nc;
+            I.nchunks = nc;
+            I.inner = models[i].inner;
+            I.pad = 0;
+            items[k] = I;
+            idx[k] = i;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_base_k += tot_a;
+            s_base_ch += tot_c;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        FusedArgs A;
+        A.items = items;
+        A.nitems = s_base_k;
+        A.chunks = chunks;
+        A.nchunks = s_base_ch;
+        A.cpart = cpart;
+        A.any_event = any_event;
+        A.bar = bar;
+        A.g_max = s_gmax < 1 ? 1 : s_gmax;
+        A.num_it0 = ctl->num_it;
+        A.pressure_schedule = s_base_k > 0 ? items[0].c.pressure_schedule : 0;
+        *args = A;
+        *any_event = 0;
+        bar->count = 0;
+        bar->gen = 0;
+        bar->error = 0;
+    }
+}
+
+// the chunk table: chunk q of the launch is chunk q - cfirst of the last
+// model whose range starts at or before q
+__global__ void fused_fill_kernel(const FusedArgs* args, FusedChunk* chunks) {
+    const FusedArgs A = *args;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < A.nchunks;
+         q += (long long)gridDim.x * blockDim.x) {
+        int lo = 0, hi = A.nitems - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (A.items[mid].cfirst <= q) lo = mid;
+            else hi = mid - 1;
+        }
+        FusedChunk ch;
+        ch.m0 = (q - A.items[lo].cfirst) * kTmaChunk;
+        ch.item = lo;
+        ch.pad = 0;
+        chunks[q] = ch;
+    }
+}
+
+// run_fused's event handling: each model's next step from its event, its
+// iterations since the last residual, whether it goes on; the residual
+// blocks of the models that need one; the loop condition
+__global__ void __launch_bounds__(kPlanThreads) fused_events_kernel(FusedCtl* ctl, FusedModel* models,
+                                                                    const FusedArgs* args, const int* idx,
+                                                                    int* act, long long* rstart,
+                                                                    cudaGraphConditionalHandle cond) {
+    __shared__ long long sh_ll[32];
+    __shared__ int s_ran, s_failed, s_active;
+    __shared__ long long s_base;
+    const FusedArgs A = *args;
+    const int na = A.nitems;
+    if (threadIdx.x == 0) {
+        s_ran = na > 0 ? A.items[0].c.st->num_it - ctl->num_it : 0;
+        s_failed = 0;
+        s_active = 0;
+        s_base = 0;
+    }
+    __syncthreads();
+    const int ran = s_ran;
+    for (int base = 0; base < na; base += kPlanThreads) {
+        const int k = base + threadIdx.x;
+        long long rb = 0;
+        if (k < na) {
+            FusedModel& M = models[idx[k]];
+            const int ev = A.items[k].c.st->event;
+            int a = 0;
+            M.inner += ran;
+            switch (ev) {
+                case EV_NONE: break;
+                case EV_CONVERGED:
+                case EV_STOP: a = ACT_APPLY; M.active = 0; break;
+                case EV_REFRESH:
+                case EV_CYCLE_END: a = ACT_APPLY | ACT_RESID; M.inner = 0; break;
+                case EV_HALVE: a = ACT_HALVE | ACT_RESID; M.inner = 0; break;
+                case EV_STOP_HALVED: a = ACT_HALVE; M.active = 0; break;
+                default: atomicExch(&s_failed, 1); M.active = 0; break;   // EV_ERROR
+            }
+            act[k] = a;
+            if (a & ACT_RESID) rb = res_blocks(A.items[k].c.L.Nc);
+        }
+        long long tot;
+        const long long p = block_inclusive_scan<long long>(rb, sh_ll, &tot);
+        if (k < na) rstart[k] = s_base + p - rb;
+        __syncthreads();
+        if (threadIdx.x == 0) s_base += tot;
+        __syncthreads();
+    }
+    // a failure ends every model, after this pass's steps (as run_fused)
+    const bool failed = s_failed != 0;
+    for (int i = threadIdx.x; i < ctl->n; i += blockDim.x) {
+        if (failed) models[i].active = 0;
+        else if (models[i].active) atomicAdd(&s_active, 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        ctl->num_it += ran;
+        ctl->launches += 1;
+        ctl->iterations += ran;
+        ctl->runs += 1;
+        ctl->resid_total = s_base;
+        if (failed) ctl->failed = 1;
+        ctl->nactive = s_active;
+        cudaGraphSetConditional(cond, (s_active > 0 && !failed && ctl->runs < kGraphMaxRuns) ? 1u : 0u);
+    }
+}
+
+// x += d (dc_apply_kernel) or the dt-halving reset (dc_halve_kernel) of the
+// models whose event asks for it, chunk by chunk
+template <class Form>
+__global__ void fused_update_kernel(const FusedArgs* args, const Form* forms, const int* idx, const int* act) {
+    const FusedArgs A = *args;
+    for (long long q = blockIdx.x; q < A.nchunks; q += gridDim.x) {
+        const FusedChunk ch = A.chunks[q];
+        const int a = act[ch.item];
+        if (!(a & (ACT_APPLY | ACT_HALVE))) continue;
+        const DcCtl& c = A.items[ch.item].c;
+        const Form F = forms[idx[ch.item]];
+        const long long Nc = c.L.Nc;
+        for (int t = threadIdx.x; t < 2 * kTmaChunk; t += blockDim.x) {
+            const int col = t >= kTmaChunk;
+            const long long m = ch.m0 + (t - col * kTmaChunk);
+            if (m >= Nc) continue;
+            if (a & ACT_APPLY) {
+                if (c.mask[col][m] & F_ACTIVE) c.X[col][m] = c.X[col][m] + (double)c.D[col][m];
+            } else {
+                F.reassemble(col, m, c.st->dt);
+                scale_cell(F, c, col, m);
+            }
+        }
+    }
+}
+
+// the residual of the models that need one: block vb of the launch is
+// residual block vb - rstart[k] of the last model k starting at or before vb
+template <class Form>
+__global__ void __launch_bounds__(kBlock) fused_residual_kernel(const FusedArgs* args, const Form* forms,
+                                                                const int* idx, const long long* rstart,
+                                                                const FusedCtl* ctl) {
+    __shared__ double sh[kBlock / 32];
+    const FusedArgs A = *args;
+    const long long total = ctl->resid_total;
+    for (long long vb = blockIdx.x; vb < total; vb += gridDim.x) {
+        int lo = 0, hi = A.nitems - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (rstart[mid] <= vb) lo = mid;
+            else hi = mid - 1;
+        }
+        const DcCtl& c = A.items[lo].c;
+        const Form F = forms[idx[lo]];
+        const long long b = vb - rstart[lo];
+        const double o2 = residual_block_cells(F, c, b, res_blocks(c.L.Nc));
+        const double s = block_sum<kBlock>(o2, sh);
+        if (threadIdx.x == 0) c.partials[b] = s;
+    }
+}
+
+// x^2 totals of the models whose residual was formed (dc_x2_kernel)
+__global__ void __launch_bounds__(kBlock) fused_x2_kernel(const FusedArgs* args, const int* act) {
+    __shared__ double sh[kBlock / 32];
+    const FusedArgs A = *args;
+    for (int k = blockIdx.x; k < A.nitems; k += gridDim.x) {
+        if (!(act[k] & ACT_RESID)) continue;
+        const DcCtl& c = A.items[k].c;
+        const int nparts = res_blocks(c.L.Nc);
+        double s = 0.0;
+        for (int b = threadIdx.x; b < nparts; b += blockDim.x) s = s + c.partials[b];
+        s = block_sum<kBlock>(s, sh);
+        if (threadIdx.x == 0) {
+            c.st->x2 = s;
+            c.st->cycles += 1;
+        }
+    }
+}
+
+static size_t fused_loop_bytes(int n) {
+    const size_t form = sizeof(PressureForm) > sizeof(TransportForm) ? sizeof(PressureForm) : sizeof(TransportForm);
+    return align256(sizeof(FusedModel) * n) + 2 * align256(sizeof(int) * n) + align256(sizeof(long long) * n) +
+           align256(sizeof(FusedArgs)) + align256(sizeof(FusedCtl)) + align256(form * n);
+}
+
+// 1: the device-driven loop (default); 0: run_fused's host loop
+int batch_loop_mode();
+
+// batch solves run by each loop since the library was loaded
+std::atomic<long long> g_graph_solves{0}, g_host_solves{0};
+
+// The fused form with the device-driven loop.  Returns 1 without doing
+// anything when the graph cannot be built (mode 0, the legacy stream, a
+// runtime without conditional nodes), so the caller runs run_fused.
+template <class Form>
+static int run_fused_graph(std::vector<BatchItem<Form>>& v, TseDcOptions* opts, void* d_ws, size_t ws_bytes,
+                           cudaStream_t stream) {
+    if (batch_loop_mode() != 1 || stream == nullptr) return 1;
+    const int n = (int)v.size();
+    long long cells = 0;
+    int Hmax = 0;
+    for (auto& it : v) {
+        cells += (long long)it.c.L.nx * it.c.L.ny * it.c.L.nz;
+        Hmax = it.c.L.H > Hmax ? it.c.L.H : Hmax;
+    }
+    if (fused_ws_bytes(n, cells) > ws_bytes) return TSE_ERR_WORKSPACE;
+    TmaStage T = tma_stage(Hmax);
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int pipes = kFusedPipes;
+    const int avail =
+        (int)std::min<size_t>((size_t)(kFusedMaxRing * pipes), fused_max_smem() / (size_t)T.bytes);
+    const int ring = avail / pipes;
+    if (ring < 2) return TSE_ERR_ARG;
+    const void* kernel = ring == 2   ? (const void*)fused_sweep_dev_kernel<2, kFusedPipes>
+                         : ring == 3 ? (const void*)fused_sweep_dev_kernel<3, kFusedPipes>
+                                     : (const void*)fused_sweep_dev_kernel<4, kFusedPipes>;
+    const int fused_threads = kTmaConsumers + 32 * pipes;
+    T.stages = ring * pipes;
+    const size_t smem = (size_t)T.stages * T.bytes;
+    if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused_max_smem()) !=
+            cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, fused_threads, smem) != cudaSuccess ||
+        per_sm < 1) {
+        cudaGetLastError();
+        return 1;
+    }
+    // the batch workspace: run_fused's areas, then the loop's own
+    const size_t nch_max = (size_t)(cells / kTmaChunk) + (size_t)n + 1;
+    char* p = (char*)d_ws;
+    FusedItem* d_items = (FusedItem*)p;
+    p += align256(sizeof(FusedItem) * n);
+    FusedChunk* d_chunks = (FusedChunk*)p;
+    p += align256(sizeof(FusedChunk) * nch_max);
+    double2* d_cpart = (double2*)p;
+    p += align256(sizeof(double2) * 8 * nch_max);
+    p += align256(sizeof(DcState) * n);
+    int* d_any = (int*)p;
+    p += 256;
+    GridBarrier* d_bar = (GridBarrier*)p;
+    p += align256(sizeof(GridBarrier)) + 256;
+    FusedModel* d_models = (FusedModel*)p;
+    p += align256(sizeof(FusedModel) * n);
+    int* d_idx = (int*)p;
+    p += align256(sizeof(int) * n);
+    int* d_act = (int*)p;
+    p += align256(sizeof(int) * n);
+    long long* d_rstart = (long long*)p;
+    p += align256(sizeof(long long) * n);
+    FusedArgs* d_args = (FusedArgs*)p;
+    p += align256(sizeof(FusedArgs));
+    FusedCtl* d_ctl = (FusedCtl*)p;
+    p += align256(sizeof(FusedCtl));
+    Form* d_forms = (Form*)p;
+
+    long long nb = (long long)sms * per_sm;
+    if (nb > (long long)nch_max) nb = (long long)nch_max;
+    const unsigned grid_small = (unsigned)(4 * sms), grid_big = (unsigned)(8 * sms);
+
+    // the graph: one WHILE node, its body captured from the stream
+    cudaGraph_t graph = nullptr, body = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaGraphConditionalHandle cond;
+    bool built = cudaGraphCreate(&graph, 0) == cudaSuccess &&
+                 cudaGraphConditionalHandleCreate(&cond, graph, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+    if (built) {
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = cond;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        built = cudaGraphAddNode(&node, graph, nullptr, 0, &cp) == cudaSuccess;
+        if (built) body = cp.conditional.phGraph_out[0];
+    }
+    if (built)
+        built = cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) ==
+                cudaSuccess;
+    if (built) {
+        fused_plan_kernel<<<1, kPlanThreads, 0, stream>>>(d_ctl, d_models, d_items, d_idx, d_args, d_chunks,
+                                                          d_cpart, d_any, d_bar);
+        fused_fill_kernel<<<grid_small, kBlock, 0, stream>>>(d_args, d_chunks);
+        cudaLaunchConfig_t lc = {};
+        lc.gridDim = dim3((unsigned)nb);
+        lc.blockDim = dim3((unsigned)fused_threads);
+        lc.dynamicSmemBytes = smem;
+        lc.stream = stream;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeCooperative;
+        at[0].val.cooperative = 1;
+        lc.attrs = at;
+        lc.numAttrs = 1;
+        const FusedArgs* a_ptr = d_args;
+        void* kargs[] = {(void*)&a_ptr, (void*)&T};
+        const cudaError_t le = cudaLaunchKernelExC(&lc, kernel, kargs);
+        fused_events_kernel<<<1, kPlanThreads, 0, stream>>>(d_ctl, d_models, d_args, d_idx, d_act, d_rstart,
+                                                            cond);
+        fused_update_kernel<Form><<<grid_big, kBlock, 0, stream>>>(d_args, d_forms, d_idx, d_act);
+        fused_residual_kernel<Form><<<grid_big, kBlock, 0, stream>>>(d_args, d_forms, d_idx, d_rstart, d_ctl);
+        fused_x2_kernel<<<grid_small, kBlock, 0, stream>>>(d_args, d_act);
+        const cudaError_t ce = cudaStreamEndCapture(stream, &body);
+        built = le == cudaSuccess && ce == cudaSuccess && cudaGetLastError() == cudaSuccess;
+    }
+    if (built) built = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+    if (!built) {
+        cudaGetLastError();
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        return 1;
+    }
+
+    // every model: state, scaled records, first residual (as run_fused)
+    int rc = TSE_OK;
+    for (auto& it : v) {
+        rc = dc_begin(it.F, it.c, it.dt, stream);
+        if (rc == TSE_OK) rc = dc_residual(it.F, it.c, stream);
+        if (rc != TSE_OK) break;
+    }
+    std::vector<FusedModel> hm(n);
+    std::vector<Form> hf(n);
+    for (int i = 0; i < n && rc == TSE_OK; ++i) {
+        memset(&hm[i], 0, sizeof(FusedModel));
+        hm[i].c = v[i].c;
+        hm[i].nchunks = (v[i].c.L.Nc + kTmaChunk - 1) / kTmaChunk;
+        hm[i].active = 1;
+        hm[i].inner = 0;
+        hf[i] = v[i].F;
+    }
+    FusedCtl hc;
+    memset(&hc, 0, sizeof(hc));
+    hc.n = n;
+    hc.nactive = n;
+    // pageable sources: staged before the calls return
+    if (rc == TSE_OK &&
+        (cudaMemcpyAsync(d_models, hm.data(), sizeof(FusedModel) * n, cudaMemcpyHostToDevice, stream) !=
+             cudaSuccess ||
+         cudaMemcpyAsync(d_forms, hf.data(), sizeof(Form) * n, cudaMemcpyHostToDevice, stream) != cudaSuccess ||
+         cudaMemcpyAsync(d_ctl, &hc, sizeof(FusedCtl), cudaMemcpyHostToDevice, stream) != cudaSuccess))
+        rc = TSE_ERR_LAUNCH;
+    const bool timing = opts && opts->timing;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    if (rc == TSE_OK && timing &&
+        (cudaEventCreate(&ev0) != cudaSuccess || cudaEventCreate(&ev1) != cudaSuccess))
+        rc = TSE_ERR_LAUNCH;
+    if (rc == TSE_OK && timing) cudaEventRecord(ev0, stream);
+    // graph launches until every model has finished: one, unless a solve needs
+    // more than kGraphMaxRuns sweep launches
+    for (int launch = 0; rc == TSE_OK; ++launch) {
+        if (cudaGraphLaunch(exec, stream) != cudaSuccess ||
+            cudaMemcpyAsync(&hc, d_ctl, sizeof(FusedCtl), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+            cudaStreamSynchronize(stream) != cudaSuccess) {
+            rc = TSE_ERR_LAUNCH;
+            break;
+        }
+        if (hc.failed || hc.nactive == 0) break;
+        if (launch >= 100000) {
+            rc = TSE_ERR_LAUNCH;
+            break;
+        }
+        hc.runs = 0;
+        if (cudaMemcpyAsync(&d_ctl->runs, &hc.runs, sizeof(int), cudaMemcpyHostToDevice, stream) != cudaSuccess)
+            rc = TSE_ERR_LAUNCH;
+    }
+    if (timing && ev0) {
+        cudaEventRecord(ev1, stream);
+        cudaEventSynchronize(ev1);
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, ev0, ev1);
+        opts->sweep_launches = hc.launches;
+        opts->sweep_iterations = hc.iterations;
+        opts->sweep_ms = ms;
+        cudaEventDestroy(ev0);
+        cudaEventDestroy(ev1);
+    }
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    g_graph_solves.fetch_add(1);
+    // status records and results of every model
+    for (auto& it : v) {
+        const int r = dc_finish(it.c, it.status, it.X_out, stream);
+        if (rc == TSE_OK) rc = r;
+    }
+    return rc;
+}
+
 }  // namespace tse
 
 using namespace tse;
+
+extern "C" int32_t tse_batch_loop_stats(int64_t* graph_solves, int64_t* host_solves) {
+    if (!graph_solves || !host_solves) return TSE_ERR_ARG;
+    *graph_solves = g_graph_solves.load();
+    *host_solves = g_host_solves.load();
+    return TSE_OK;
+}
 
 extern "C" size_t tse_batch_workspace_bytes(int32_t n, int64_t total_cells) {
     if (n < 1) n = 1;
@@ -871,6 +1398,9 @@ extern "C" int32_t tse_compute_P_dc_batch(const TseBatchPressure* items, int32_t
         v[i].cells = 2 * S.L.Nc;
     }
     if (opts && opts->max_blocks > 0) return launch_batch(v, opts, d_batch_ws, batch_ws_bytes, stream);
+    const int g = run_fused_graph(v, opts, d_batch_ws, batch_ws_bytes, stream);
+    if (g != 1) return g;
+    g_host_solves.fetch_add(1);
     return run_fused(v, opts, d_batch_ws, batch_ws_bytes, stream);
 }
 
@@ -900,6 +1430,9 @@ extern "C" int32_t tse_compute_C_dc_batch(const TseBatchSpecies* items, int32_t 
         v[i].cells = 2 * S.L.Nc;
     }
     if (opts && opts->max_blocks > 0) return launch_batch(v, opts, d_batch_ws, batch_ws_bytes, stream);
+    const int g = run_fused_graph(v, opts, d_batch_ws, batch_ws_bytes, stream);
+    if (g != 1) return g;
+    g_host_solves.fetch_add(1);
     return run_fused(v, opts, d_batch_ws, batch_ws_bytes, stream);
 }
 
@@ -929,5 +1462,8 @@ extern "C" int32_t tse_compute_T_dc_batch(const TseBatchHeat* items, int32_t n,
         v[i].cells = 2 * S.L.Nc;
     }
     if (opts && opts->max_blocks > 0) return launch_batch(v, opts, d_batch_ws, batch_ws_bytes, stream);
+    const int g = run_fused_graph(v, opts, d_batch_ws, batch_ws_bytes, stream);
+    if (g != 1) return g;
+    g_host_solves.fetch_add(1);
     return run_fused(v, opts, d_batch_ws, batch_ws_bytes, stream);
 }

@@ -45,7 +45,6 @@ constexpr int kSweepBlock = TSE_SWEEP_BLOCK;
 #ifndef TSE_TMA_PREFETCH
 #define TSE_TMA_PREFETCH 1   // 1: a phase's own parts are copied before its grid barrier
 #endif
-constexpr int kResBlocks = 2048;   // fixed grid of the residual kernel (deterministic sums)
 
 // Pipelines of the staged sweep: each has its own producer warp, its own ring
 // of stages and its own consumer group, and takes every PIPES-th chunk of the
@@ -89,24 +88,7 @@ __global__ void dc_halve_kernel(Form F, DcCtl c) {
 template <class Form>
 __global__ void __launch_bounds__(kBlock) dc_residual_kernel(Form F, DcCtl c) {
     __shared__ double sh[kBlock / 32];
-    const long long Nc = c.L.Nc;
-    double o2 = 0.0;
-    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < 2 * Nc;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int col = t >= Nc;
-        const long long m = t - col * Nc;
-        const uint8_t f = c.mask[col][m];
-        const double x = c.X[col][m];
-        o2 = o2 + x * x;
-        float rp = 0.0f;
-        if (f & F_ACTIVE) {
-            const double den = F.den(col, m);
-            const double r = F.sum(col, m, f, c.X[1 - col]) - den * x;
-            rp = (float)(r / den);
-        }
-        c.K[col][6 * c.Ncal + m] = rp;
-        c.D[col][m] = 0.0f;
-    }
+    const double o2 = residual_block_cells(F, c, blockIdx.x, gridDim.x);
     const double b = block_sum<kBlock>(o2, sh);
     if (threadIdx.x == 0) c.partials[blockIdx.x] = b;
 }
@@ -671,7 +653,7 @@ static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, 
     int prev_it = 0;
     int rc = TSE_OK;
     for (;;) {
-        const unsigned rb = (unsigned)std::min<long long>(kResBlocks, (cells2 + kBlock - 1) / kBlock);
+        const unsigned rb = (unsigned)res_blocks(S.L.Nc);
         dc_residual_kernel<<<rb, kBlock, 0, stream>>>(S.F, c);
         dc_x2_kernel<<<1, kBlock, 0, stream>>>(c, (int)rb);
         void* args[] = {(void*)&c};
@@ -758,8 +740,7 @@ int dc_begin(const Form& F, const DcCtl& c, double dt, cudaStream_t stream) {
 
 template <class Form>
 int dc_residual(const Form& F, const DcCtl& c, cudaStream_t stream) {
-    const long long cells2 = 2 * c.L.Nc;
-    const unsigned rb = (unsigned)std::min<long long>(kResBlocks, (cells2 + kBlock - 1) / kBlock);
+    const unsigned rb = (unsigned)res_blocks(c.L.Nc);
     dc_residual_kernel<<<rb, kBlock, 0, stream>>>(F, c);
     dc_x2_kernel<<<1, kBlock, 0, stream>>>(c, (int)rb);
     return cudaGetLastError() == cudaSuccess ? TSE_OK : TSE_ERR_LAUNCH;

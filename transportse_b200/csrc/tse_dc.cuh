@@ -61,6 +61,41 @@ __device__ __forceinline__ void scale_cell(const Form& F, const DcCtl& c, int co
     }
 }
 
+// FP64 residual of the correction equation: fixed grid of the residual
+// kernel (deterministic sums); one block's share of a model's cells
+constexpr int kResBlocks = 2048;
+
+__host__ __device__ inline int res_blocks(long long Nc) {
+    const long long rb = (2 * Nc + kBlock - 1) / kBlock;
+    return (int)(rb < kResBlocks ? rb : kResBlocks);
+}
+
+// r' = (sum(x) - Den x) / Den, d = 0 for the cells t = b*kBlock + tid +
+// s*nblocks*kBlock of both colours (t < 2 Nc) as residual block b of nblocks;
+// returns this thread's sum of x^2 (all cells, active or not)
+template <class Form>
+__device__ __forceinline__ double residual_block_cells(const Form& F, const DcCtl& c, long long b,
+                                                       long long nblocks) {
+    const long long Nc = c.L.Nc;
+    double o2 = 0.0;
+    for (long long t = b * kBlock + threadIdx.x; t < 2 * Nc; t += nblocks * kBlock) {
+        const int col = t >= Nc;
+        const long long m = t - col * Nc;
+        const uint8_t f = c.mask[col][m];
+        const double x = c.X[col][m];
+        o2 = o2 + x * x;
+        float rp = 0.0f;
+        if (f & F_ACTIVE) {
+            const double den = F.den(col, m);
+            const double r = F.sum(col, m, f, c.X[1 - col]) - den * x;
+            rp = (float)(r / den);
+        }
+        c.K[col][6 * c.Ncal + m] = rp;
+        c.D[col][m] = 0.0f;
+    }
+    return o2;
+}
+
 // The coefficients of a cell are one 24-byte record (three 8-byte loads
 // from one address); the z-neighbours dq[m-1], dq[m+1] are the dq[m] values
 // the adjacent lanes load (consecutive lanes hold consecutive m), fetched
