@@ -85,7 +85,15 @@ def parse_args():
     ap.add_argument("--requests", type=int, default=40, help="serving: requests")
     ap.add_argument("--rate", type=float, default=20.0, help="serving: arrivals per second")
     ap.add_argument("--slots", type=int, default=8, help="serving: concurrent models")
+    ap.add_argument("--batch-loop", choices=("device", "host"), default="device",
+                    help="ensemble/serving, batched: the fused form's loop (device: one CUDA "
+                         "graph per batch solve; host: a host round trip per sweep launch)")
     return ap.parse_args()
+
+
+def set_batch_loop(a):
+    from transportse_b200 import _native
+    _native.lib().tse_set_batch_loop(1 if a.batch_loop == "device" else 0)
 
 
 def bench_ensemble(a):
@@ -95,6 +103,7 @@ def bench_ensemble(a):
     models in one launch, cluster size autotuned on a sample; unbatched:
     concurrency and cycle length autotuned on a sample."""
     import torch
+    set_batch_loop(a)
     from transportse_b200 import workloads
     from transportse_b200.ensemble import Ensemble, autotune
     dev = torch.device("cuda:0")
@@ -135,7 +144,7 @@ def bench_ensemble(a):
         "setup_s": st["setup_s"], "step_s": st["step_s"],
         "with_setup_cell_updates_per_s": st["cell_updates_per_s"],
         "wall_s": st["wall_s"], "batched": batched, "cluster": cl, "concurrency": st["concurrency"],
-        "dc_cycle": cyc, "max_blocks": st["max_blocks"], "batch": st["batch"],
+        "dc_cycle": cyc, "max_blocks": st["max_blocks"], "batch_loop": a.batch_loop, "batch": st["batch"],
         "autotune": tune, "clocks": clk}))
 
 
@@ -193,6 +202,7 @@ def bench_serving(a):
     a.steps coupled flow/heat/species steps; HBM-budget admission, slots run
     concurrently; p50/p99 latency and aggregate cell-update rate."""
     import torch
+    set_batch_loop(a)
     from transportse_b200 import workloads
     from transportse_b200.serving import Server, poisson_trace
     dev = torch.device("cuda:0")
@@ -212,8 +222,8 @@ def bench_serving(a):
                                "%d steps each, %d slots, HBM budget %.0f GB"
                                % (a.requests, a.rate, nmax, a.steps, a.slots, budget / 1e9)},
         "latency_p50_s": st["p50_s"], "latency_p99_s": st["p99_s"], "latency_mean_s": st["mean_s"],
-        "makespan_s": st["makespan_s"], "batched": st["batched"], "batch": st["batch"],
-        "clocks": clk}))
+        "makespan_s": st["makespan_s"], "batched": st["batched"], "batch_loop": a.batch_loop,
+        "batch": st["batch"], "clocks": clk}))
 
 
 def shape_of(a):
