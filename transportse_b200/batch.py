@@ -5,8 +5,10 @@ full time-step driver on its own thread and CUDA stream.  When a model
 reaches a mixed-precision pressure / species / heat solve, ``Model._solve``
 hands the call to the ``BatchGate`` it is attached to and waits.  Once every
 live member is waiting at a solve, the gate issues the waiting calls as one
-``tse_compute_*_dc_batch`` launch per solve kind -- one thread-block cluster
-per model, all models of the kind side by side -- and releases the members.
+``tse_compute_*_dc_batch`` call per solve kind -- by default the fused form:
+every model's cells in one cooperative sweep, the loop around the sweeps run
+on the device as one CUDA graph (``cluster > 0``: one thread-block cluster
+per model instead) -- and releases the members.
 Members that are between solves keep the gate open (it never launches a
 partial batch while one of them may still arrive), members that finish
 leave, and new ones join between steps: continuous batching.

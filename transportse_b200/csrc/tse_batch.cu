@@ -1,5 +1,10 @@
-// Batched mixed-precision solves: many independent models in one persistent
-// launch, one thread-block cluster per model.
+// Batched mixed-precision solves of many independent models, in two forms.
+//
+// The fused form (the default; further down): every model's cells in one
+// cooperative sweep sharing the colour-phase barriers, the loop around the
+// sweeps (plan, events, residuals) run on the device as one CUDA graph.
+//
+// The cluster form (opts->max_blocks > 0): one thread-block cluster per model.
 //
 // For a small model the whole-GPU solve (tse_dc.cu) is bound by its two
 // device-wide barriers per red+black iteration, not by memory: a 124K-cell

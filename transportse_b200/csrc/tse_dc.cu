@@ -236,7 +236,7 @@ __global__ void __launch_bounds__(kSweepBlock, kSweepMinBlocks) dc_sweep_kernel(
     }
 }
 
-// ------------------------------------------------ FP32 sweeps, TMA-staged
+// ------------------------------------------------ FP32 sweeps, bulk-copy staged
 // (the staging pieces are in tse_dc.cuh)
 template <int RING, int PIPES>
 __global__ void __launch_bounds__(DcLayout<PIPES>::kThreads, DcLayout<PIPES>::kMinBlocks)
@@ -547,7 +547,7 @@ static int sweep_blocks(long long Nc, int cap) {
 }
 
 #ifndef TSE_SWEEP_TMA
-#define TSE_SWEEP_TMA 1   // 1: TMA-staged sweeps where the stages fit in shared memory
+#define TSE_SWEEP_TMA 1   // 1: bulk-copy staged sweeps where the stages fit in shared memory
 #endif
 // dynamic shared memory ceiling of the staged sweep: the device's per-block
 // opt-in limit less the kernel's static arrays and a margin

@@ -188,7 +188,7 @@ inline void dc_carve(SolveSetup<Form>& S, DcCtl& c, int x_index) {
     c.bar = S.bar;
 }
 
-// ------------------------------------------------ FP32 sweeps, TMA-staged
+// ------------------------------------------------ FP32 sweeps, bulk-copy staged
 // The same iterations as dc_sweep_kernel, with the memory side rebuilt for
 // bytes in flight: the cells of a colour are cut into chunks of kTmaChunk,
 // block b takes chunks b, b + G, ...; for each chunk one thread issues bulk

@@ -5,8 +5,9 @@ slots and device memory free up, keeps each admitted model's state resident
 on the GPU until its last step, and runs the admitted models concurrently,
 one host thread and CUDA stream per slot.  With ``batched`` (the default for
 the mixed-precision form) the slots' solves meet at a ``BatchGate``: each
-kind of solve of all admitted models runs as one launch, one thread-block
-cluster per model; otherwise the cooperative sweep kernels of concurrent
+kind of solve of all admitted models runs as one batched call (the fused
+form: one cooperative sweep over every model's cells, its loop one CUDA
+graph on the device); otherwise the cooperative sweep kernels of concurrent
 solves each take a share of the SMs.  A request that arrives while others are
 running starts as soon as a slot is free and its state fits the HBM budget,
 and joins the next batch of solves -- continuous batching at the granularity
