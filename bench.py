@@ -85,6 +85,9 @@ def parse_args():
     ap.add_argument("--requests", type=int, default=40, help="serving: requests")
     ap.add_argument("--rate", type=float, default=20.0, help="serving: arrivals per second")
     ap.add_argument("--slots", type=int, default=8, help="serving: concurrent models")
+    ap.add_argument("--gate", choices=("eager", "lockstep"), default="lockstep",
+                    help="serving, batched: issue a batch as soon as a solve waits and the GPU "
+                         "is free (eager), or once every running request waits (lockstep)")
     ap.add_argument("--batch-loop", choices=("device", "host"), default="device",
                     help="ensemble/serving, batched: the fused form's loop (device: one CUDA "
                          "graph per batch solve; host: a host round trip per sweep launch)")
@@ -213,7 +216,7 @@ def bench_serving(a):
     clocks = ClockSampler(0)
     clocks.start()
     reqs, st = Server(device=dev, slots=a.slots, hbm_budget=budget, batched=not a.streams,
-                      cluster=a.cluster).replay(trace)
+                      cluster=a.cluster, eager=a.gate == "eager").replay(trace)
     clk = clocks.stop()
     print(json.dumps({
         "metric": "SOR cell-updates/s", "value": st["cell_updates_per_s"], "unit": "cell-updates/s",
@@ -222,7 +225,8 @@ def bench_serving(a):
                                "%d steps each, %d slots, HBM budget %.0f GB"
                                % (a.requests, a.rate, nmax, a.steps, a.slots, budget / 1e9)},
         "latency_p50_s": st["p50_s"], "latency_p99_s": st["p99_s"], "latency_mean_s": st["mean_s"],
-        "makespan_s": st["makespan_s"], "batched": st["batched"], "batch_loop": a.batch_loop,
+        "makespan_s": st["makespan_s"], "batched": st["batched"], "gate": a.gate,
+        "batch_loop": a.batch_loop,
         "batch": st["batch"], "clocks": clk}))
 
 

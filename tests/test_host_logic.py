@@ -152,6 +152,50 @@ def test_batch_gate_launches_when_every_member_waits(monkeypatch):
     assert gate.members == 0 and gate.running == 0
 
 
+def test_eager_batch_gate_overlaps_host_work_with_a_running_batch(monkeypatch):
+    """BatchGate(eager=True): a solve goes out as soon as it waits and no batch
+    runs, without waiting for the other members; the gate's lock is free while
+    a batch runs, so a member submits meanwhile and its solve forms the next
+    batch once the running one ends."""
+    import threading
+    import time
+    from transportse_b200 import batch as B
+
+    launched = []
+
+    def fake_launch(self, reqs):
+        launched.append(sorted(r.name for r in reqs))
+        time.sleep(0.2)          # the batch occupies the GPU
+
+    monkeypatch.setattr(B.BatchGate, "_launch", fake_launch)
+    monkeypatch.setattr(B.torch.cuda, "current_stream", lambda device=None: None)
+    gate = B.BatchGate("cpu", eager=True)
+    done = {}
+
+    def member(name, delay):
+        try:
+            time.sleep(delay)
+            gate.submit(name, None, None, None, None, 0, 128)
+            done[name] = time.perf_counter()
+        finally:
+            gate.leave()
+
+    for _ in range(3):
+        gate.join()
+    t0 = time.perf_counter()
+    ths = [threading.Thread(target=member, args=a, daemon=True)
+           for a in (("compute_P", 0.0), ("compute_T", 0.05), ("compute_C", 0.1))]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join(timeout=10)
+    assert not any(t.is_alive() for t in ths)
+    # the first solve went out alone; the two that arrived during it, together
+    assert launched == [["compute_P"], ["compute_C", "compute_T"]]
+    assert done["compute_P"] - t0 < 0.35 < done["compute_T"] - t0
+    assert gate.members == 0 and gate.running == 0 and not gate.launching
+
+
 def test_snapshot_rule_matches_the_oracle(tmp_path):
     """driver.Snapshots (product) and oracle.driver.Plots (restatement of
     tse.py:312-329) give the same dt sequence and files, including a plot time

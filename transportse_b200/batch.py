@@ -51,17 +51,28 @@ class _Request:
 
 class BatchGate:
     """Collects the mixed-precision solves of the member models and launches
-    them together.  ``cluster``: CTAs per model (0: the library default, 8).
+    them together.  ``cluster``: CTAs per model (0: the fused form).
+
+    ``eager``: when to issue a batch.  False (lock step): once every live
+    member waits at a solve -- the largest batches, for ensembles whose
+    members step together.  True: as soon as a solve waits and no batch is
+    on the GPU -- the members that arrive while a batch runs form the next
+    one, so their host work between solves overlaps the GPU's work; for
+    serving, whose requests differ in size and arrive over time.  Either way
+    the gate's lock is free while a batch runs, and a model's results do not
+    depend on which batch it was in.
 
     Use ``with gate.member():`` around a member thread's work, and attach the
     gate to its model (``Model.batch_gate = gate``)."""
 
-    def __init__(self, device=None, cluster=0):
+    def __init__(self, device=None, cluster=0, eager=False):
         self.device = torch.device(device if device is not None else "cuda")
         self.cluster = int(cluster)
-        self.cv = threading.Condition()
+        self.eager = bool(eager)
+        self.cv = threading.Condition(threading.Lock())
         self.members = 0
         self.running = 0
+        self.launching = False
         self.pending = []
         self.streams = {}
         self.ws = {}
@@ -104,26 +115,36 @@ class BatchGate:
                 raise RuntimeError("BatchGate.submit from a thread that has not joined the gate")
             self.pending.append(req)
             self.running -= 1
+            # a waiting member issues the next batch once it may go out (its
+            # own solve among the batch's), then returns to its model
             self._maybe_flush()
             while not req.done:
                 self.cv.wait()
+                self._maybe_flush()
         if req.error is not None:
             raise req.error
 
     def _maybe_flush(self):
-        # caller holds self.cv
-        if self.running > 0 or not self.pending:
-            return
-        reqs, self.pending = self.pending, []
-        try:
-            self._launch(reqs)
-        except Exception as e:   # every waiting member sees the failure
+        # caller holds self.cv; it is released while the batch runs.  The
+        # requests that arrive meanwhile wait; the end of the batch wakes
+        # their threads, one of which issues them
+        if self.pending and not self.launching and (self.eager or self.running == 0):
+            reqs, self.pending = self.pending, []
+            self.launching = True
+            self.cv.release()
+            err = None
+            try:
+                self._launch(reqs)
+            except Exception as e:   # every waiting member sees the failure
+                err = e
+            finally:
+                self.cv.acquire()
+                self.launching = False
             for r in reqs:
-                r.error = e
-        for r in reqs:
-            r.done = True
-        self.running += len(reqs)
-        self.cv.notify_all()
+                r.error = err
+                r.done = True
+            self.running += len(reqs)
+            self.cv.notify_all()
 
     def _stream(self, key):
         s = self.streams.get(key)
