@@ -64,6 +64,16 @@ struct DcLayout {
 };
 
 // ------------------------------------------------------------ FP64 kernels
+// a solve's state record at its start: all zero but dt and diff (written on
+// the device, so starting a solve queues no host-memory copy)
+__global__ void dc_init_state_kernel(DcState* st, double dt) {
+    DcState s;
+    memset(&s, 0, sizeof(s));
+    s.dt = dt;
+    s.diff = 1e100;
+    *st = s;
+}
+
 // K'_q = k_q / Den for every cell (at the start and after dt halving)
 template <class Form>
 __global__ void dc_scale_kernel(Form F, DcCtl c) {
@@ -616,14 +626,11 @@ static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, 
     c.sor = (float)sor;
     const long long dlen = dc_delta_len(S.L, S.Ncal);
     float* dbase = c.D[0] - dc_margin(S.L);
-    DcState init;
-    memset(&init, 0, sizeof(init));
-    init.dt = dt;
-    init.diff = 1e100;
     // the margins must read as 0 (kernels rewrite the interior only)
-    if (cudaMemsetAsync(dbase, 0, (size_t)2 * dlen * sizeof(float), stream) != cudaSuccess ||
-        cudaMemcpyAsync(c.st, &init, sizeof(DcState), cudaMemcpyHostToDevice, stream) != cudaSuccess)
+    if (cudaMemsetAsync(dbase, 0, (size_t)2 * dlen * sizeof(float), stream) != cudaSuccess)
         return TSE_ERR_LAUNCH;
+    dc_init_state_kernel<<<1, 1, 0, stream>>>(c.st, dt);
+    if (cudaGetLastError() != cudaSuccess) return TSE_ERR_LAUNCH;
     const long long cells2 = 2 * S.L.Nc;
     const unsigned gcells = (unsigned)((cells2 + kBlock - 1) / kBlock);
     TmaStage T = tma_stage(S.L.H);
@@ -724,15 +731,12 @@ static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, 
 // and finish (status record + natural-layout result).
 template <class Form>
 int dc_begin(const Form& F, const DcCtl& c, double dt, cudaStream_t stream) {
-    DcState init;
-    memset(&init, 0, sizeof(init));
-    init.dt = dt;
-    init.diff = 1e100;
     float* dbase = c.D[0] - dc_margin(c.L);
     const long long dlen = dc_delta_len(c.L, c.Ncal);
-    if (cudaMemsetAsync(dbase, 0, (size_t)2 * dlen * sizeof(float), stream) != cudaSuccess ||
-        cudaMemcpyAsync(c.st, &init, sizeof(DcState), cudaMemcpyHostToDevice, stream) != cudaSuccess)
+    if (cudaMemsetAsync(dbase, 0, (size_t)2 * dlen * sizeof(float), stream) != cudaSuccess)
         return TSE_ERR_LAUNCH;
+    dc_init_state_kernel<<<1, 1, 0, stream>>>(c.st, dt);
+    if (cudaGetLastError() != cudaSuccess) return TSE_ERR_LAUNCH;
     const unsigned g = (unsigned)((2 * c.L.Nc + kBlock - 1) / kBlock);
     dc_scale_kernel<<<g, kBlock, 0, stream>>>(F, c);
     return cudaGetLastError() == cudaSuccess ? TSE_OK : TSE_ERR_LAUNCH;
