@@ -196,6 +196,53 @@ def test_eager_batch_gate_overlaps_host_work_with_a_running_batch(monkeypatch):
     assert gate.members == 0 and gate.running == 0 and not gate.launching
 
 
+@pytest.mark.parametrize("eager", [False, True])
+def test_batch_gate_failure_reaches_its_batch_and_the_gate_recovers(monkeypatch, eager):
+    """A batched call that raises: every member of that batch gets the error,
+    the gate's lock and counters are left consistent, and later solves go out
+    normally."""
+    import threading
+    from transportse_b200 import batch as B
+
+    calls = []
+
+    def fake_launch(self, reqs):
+        calls.append(len(reqs))
+        if len(calls) == 1:
+            raise RuntimeError("launch failed")
+
+    monkeypatch.setattr(B.BatchGate, "_launch", fake_launch)
+    monkeypatch.setattr(B.torch.cuda, "current_stream", lambda device=None: None)
+    gate = B.BatchGate("cpu", eager=eager)
+    errors, ok = [], []
+    start = threading.Barrier(2)
+
+    def member():
+        try:
+            start.wait()
+            for k in range(2):
+                try:
+                    gate.submit("compute_P", None, None, None, None, 0, 128)
+                    ok.append(k)
+                except RuntimeError as e:
+                    errors.append((k, str(e)))
+        finally:
+            gate.leave()
+
+    for _ in range(2):
+        gate.join()
+    ths = [threading.Thread(target=member, daemon=True) for _ in range(2)]
+    for t in ths:
+        t.start()
+    for t in ths:
+        t.join(timeout=10)
+    assert not any(t.is_alive() for t in ths)
+    # whoever was in the first batch saw its failure; every later solve ran
+    assert errors and all(k == 0 and msg == "launch failed" for k, msg in errors)
+    assert len(errors) == calls[0] and len(ok) == 4 - len(errors)
+    assert gate.members == 0 and gate.running == 0 and not gate.launching and not gate.pending
+
+
 def test_snapshot_rule_matches_the_oracle(tmp_path):
     """driver.Snapshots (product) and oracle.driver.Plots (restatement of
     tse.py:312-329) give the same dt sequence and files, including a plot time
