@@ -243,6 +243,47 @@ def test_batch_gate_failure_reaches_its_batch_and_the_gate_recovers(monkeypatch,
     assert gate.members == 0 and gate.running == 0 and not gate.launching and not gate.pending
 
 
+def _last_at_or_before(starts, q):
+    """The device loop's binary search (fused_fill_kernel,
+    fused_residual_kernel): the last index k with starts[k] <= q."""
+    lo, hi = 0, len(starts) - 1
+    while lo < hi:
+        mid = (lo + hi + 1) >> 1
+        if starts[mid] <= q:
+            lo = mid
+        else:
+            hi = mid - 1
+    return lo
+
+
+def test_device_loop_index_maps_cover_every_chunk_and_residual_block():
+    """The batched device loop maps chunk q of a launch to its model through
+    the models' chunk ranges, and residual block vb to its model through the
+    residual prefix sums, in which models without a residual this pass have
+    no blocks: every chunk and every block lands in exactly one model, at the
+    right offset, never in a model with an empty range."""
+    import random
+    rng = random.Random(17)
+    for _ in range(300):
+        n = rng.randint(1, 40)
+        nchunks = [rng.randint(1, 9) for _ in range(n)]          # every model >= 1 chunk
+        cfirst = [sum(nchunks[:k]) for k in range(n)]
+        seen = []
+        for q in range(sum(nchunks)):
+            k = _last_at_or_before(cfirst, q)
+            assert cfirst[k] <= q < cfirst[k] + nchunks[k]
+            seen.append((k, q - cfirst[k]))
+        assert seen == [(k, j) for k in range(n) for j in range(nchunks[k])]
+        rb = [rng.choice([0, 0, rng.randint(1, 2048)]) for _ in range(n)]   # residual blocks
+        rstart = [sum(rb[:k]) for k in range(n)]
+        blocks = []
+        for vb in range(sum(rb)):
+            k = _last_at_or_before(rstart, vb)
+            assert rb[k] > 0 and 0 <= vb - rstart[k] < rb[k]
+            blocks.append((k, vb - rstart[k]))
+        assert blocks == [(k, b) for k in range(n) for b in range(rb[k])]
+
+
 def test_snapshot_rule_matches_the_oracle(tmp_path):
     """driver.Snapshots (product) and oracle.driver.Plots (restatement of
     tse.py:312-329) give the same dt sequence and files, including a plot time
