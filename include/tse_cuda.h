@@ -172,8 +172,9 @@ int32_t tse_compute_T_dc(const TseGrid *grid, const TseHeatArgs *args,
  * event time (the cluster form writes nothing).
  *   opts->max_blocks <= 0: fused form -- every model's cells in one
  *     cooperative sweep sharing its barriers (models that finish drop out);
- *     the call synchronises the stream once per launch and returns when
- *     every solve is done;
+ *     the loop around the sweeps runs on the device as one CUDA graph launch
+ *     (tse_set_batch_loop: or on the host, one stream synchronisation per
+ *     sweep launch); the call returns when every solve is done;
  *   opts->max_blocks > 0: cluster form -- one persistent launch with one
  *     thread-block cluster of max_blocks CTAs (at most 16) per model; the
  *     call returns after queueing the work, nothing is read back.
