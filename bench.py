@@ -450,7 +450,7 @@ def roofline(res, precision, peak, peak_kind):
         if not res["n_s"]:
             return None
         units, ms, n = res["s_units"], res["s_ms"], res["n_s"]
-        name = "dc_sweep_tma_kernel<4> (FP32 correction sweeps, bulk-copy pipelines)"
+        name = "dc_sweep_tma_kernel<4, 2> (FP32 correction sweeps, bulk-copy pipelines)"
     else:
         if not res["n_p"]:
             return None
