@@ -392,10 +392,16 @@ def timed_steps(ctx, sim, steps, clocks=None):
     ms = e0.elapsed_time(e1)
     updates = sum(M.cell_updates[k] - cu0[k] for k in cu0)
     p_units, p_ms, n_p, active_p = 0.0, 0.0, 0, 0
+    by = {}   # per solve kind: cell-updates, event ms of the solve calls, calls
     for kind, s0, s1, nit, active in M.timed:
+        ms_k = s0.elapsed_time(s1)
+        b = by.setdefault(kind, [0.0, 0.0, 0])
+        b[0] += float(nit) * active
+        b[1] += ms_k
+        b[2] += 1
         if kind == "P":
             p_units += float(nit) * active
-            p_ms += s0.elapsed_time(s1)
+            p_ms += ms_k
             n_p += 1
             active_p = active
     # mixed-precision form: the FP32 sweep kernel's own launches (events
@@ -406,7 +412,11 @@ def timed_steps(ctx, sim, steps, clocks=None):
             s_units += float(iters) * active_p
             s_ms += sms
             n_s += launches
+    rates = {k: {"cell_updates": u, "ms": t, "calls": n,
+                 "cell_updates_per_s": u / (t / 1e3) if t > 0 else None}
+             for k, (u, t, n) in sorted(by.items())}
     return {"ms": ms, "updates": updates, "launches": M.launches - launches0, "clocks": clk,
+            "rates_by_solve": rates,
             "iterations": {k: sim.counters[k] - it0[k] for k in it0},
             "p_units": p_units, "p_ms": p_ms, "n_p": n_p,
             "s_units": s_units, "s_ms": s_ms, "n_s": n_s}
@@ -605,6 +615,9 @@ def main():
                        "parallelism": "replicas" if world > 1 else "single",
                        "l2": "working set > L2 (no flush)"},
             "gpu_launches": int(res["launches"]), "clocks": res["clocks"], "e2e": e2e,
+            # pressure SOR / species / heat separately: each solve call's event
+            # time (sweeps, residuals, set-up) and its cell-updates
+            "rates_by_solve": res["rates_by_solve"],
             "roofline": roof, "fp64_plain": fp64, "cpu_baseline": cpu}))
     if world > 1:
         dist.barrier()
