@@ -91,27 +91,60 @@ def parse_args():
     ap.add_argument("--batch-loop", choices=("device", "host"), default="device",
                     help="ensemble/serving, batched: the fused form's loop (device: one CUDA "
                          "graph per batch solve; host: a host round trip per sweep launch)")
+    ap.add_argument("--ensemble-models", type=int, default=512,
+                    help="default run: models of the batched-ensemble key (0: leave it out)")
+    ap.add_argument("--ensemble-steps", type=int, default=10,
+                    help="default run: time steps of every model of the ensemble key")
+    ap.add_argument("--serving-requests", type=int, default=40,
+                    help="default run: requests of the serving key (0: leave it out)")
+    ap.add_argument("--serving-steps", type=int, default=50,
+                    help="default run: time steps of every request of the serving key")
+    ap.add_argument("--serving-n-max", type=int, default=192,
+                    help="default run: largest cubic edge of the serving key's requests")
     return ap.parse_args()
 
 
-def set_batch_loop(a):
-    from transportse_b200 import _native
-    _native.lib().tse_set_batch_loop(1 if a.batch_loop == "device" else 0)
+def with_loop(runner, a):
+    """The --batch-loop choice on a runner's batch gate (per call, through
+    TseDcOptions.host_loop)."""
+    if getattr(runner, "gate", None) is not None:
+        runner.gate.host_loop = a.batch_loop == "host"
+    return runner
 
 
-def bench_ensemble(a):
-    """Ensemble of independent models (log-uniform 32-128 per axis, lognormal
-    K, one source/sink, one species plus heat), FP32+DC, a.steps time steps
+def batched_roofline(units, st, peak, peak_kind):
+    """Roofline of the batched form from a batch gate's statistics: the fused
+    sweep kernel's own time (global timer inside the device-driven loop's
+    graph) and the loop around it, at the algorithmic 29 bytes per
+    cell-update of the FP32 correction sweep."""
+    sw = (st or {}).get("sweeps") or {}
+    ms = sum(v["ms"] for v in sw.values())
+    loop_ms = sum(v.get("loop_ms", 0.0) for v in sw.values())
+    launches = sum(v["launches"] for v in sw.values())
+    if ms <= 0 or launches == 0:
+        return None
+    b = ALG_BYTES["fp32dc"]
+    achieved = units * b / (ms / 1e3) / 1e9
+    return {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "traffic": None,
+            "kernel": "fused_sweep_dev_kernel<4, 2> (all models' FP32 correction sweeps in one "
+                      "cooperative launch, inside the device-driven loop)",
+            "algorithmic_bytes_per_cell_update": b, "launches": launches,
+            "ms_per_launch": ms / launches, "cell_updates_per_launch": units / launches,
+            "loop_frac": (units * b / (loop_ms / 1e3) / 1e9 / peak) if loop_ms > 0 else None,
+            "peak_source": peak_kind}
+
+
+def ensemble_run(a, dev, models, steps, nmax=128, clocks=True):
+    """Ensemble of independent models (log-uniform 32-nmax per axis, lognormal
+    K, one source/sink, one species plus heat), FP32+DC, ``steps`` time steps
     each.  Batched (default): every model resident, each kind of solve of all
-    models in one launch, cluster size autotuned on a sample; unbatched:
+    models in one fused launch sequence (the device-driven loop), the
+    correction-cycle length autotuned on a sample; unbatched (--streams):
     concurrency and cycle length autotuned on a sample."""
-    import torch
-    set_batch_loop(a)
     from transportse_b200 import workloads
     from transportse_b200.ensemble import Ensemble, autotune
-    dev = torch.device("cuda:0")
-    nmax = a.n_max or 128
-    cfgs = [workloads.ensemble_member(seed=1000 + i, n_max=nmax) for i in range(a.models)]
+    cfgs = [workloads.ensemble_member(seed=1000 + i, n_max=nmax) for i in range(models)]
     tune = None
     batched = not a.streams
     conc = cyc = cl = None
@@ -130,25 +163,41 @@ def bench_ensemble(a):
         else:
             conc = a.concurrency
         kw = {"batched": False, "concurrency": conc}
-    clocks = ClockSampler(0)
-    clocks.start()
-    _, st = Ensemble(cfgs, device=dev, precision="fp32dc", dc_cycle=cyc, **kw).run(a.steps, keep=())
-    clk = clocks.stop()
+    sampler = ClockSampler(0) if clocks else None
+    if sampler:
+        sampler.start()
+    _, st = with_loop(Ensemble(cfgs, device=dev, precision="fp32dc", dc_cycle=cyc, **kw), a).run(
+        steps, keep=())
+    clk = sampler.stop() if sampler else None
     cells = [c.nx * c.ny * c.nz for c in cfgs]
     value = st["stepping_cell_updates_per_s"] or st["cell_updates_per_s"]
-    print(json.dumps({
+    peak, peak_kind = measured_peak()
+    roof = batched_roofline(st["cell_updates"], st["batch"], peak, peak_kind) if batched else None
+    if roof is not None and st["step_s"]:
+        # the whole batched form over the stepping phase: sweeps, the loop
+        # around them, the transport solves and every model's host steps
+        roof["form_frac"] = value * ALG_BYTES["fp32dc"] / 1e9 / peak
+    return {
         "metric": "SOR cell-updates/s", "value": value, "unit": "cell-updates/s",
-        "n_gpus": 1, "steps": a.steps, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "ensemble of %d models, axes log-uniform 32-%d, %d steps each, "
                                "FP32 sweeps + FP64 defect correction; value = cell-updates over "
                                "the stepping phase (one-time model set-up in setup_s)"
-                               % (a.models, nmax, a.steps),
+                               % (models, nmax, steps),
+                   "models": models, "steps": steps,
                    "cells_total": int(sum(cells)), "cells_max": int(max(cells))},
-        "setup_s": st["setup_s"], "step_s": st["step_s"],
+        "setup_s": st["setup_s"], "step_s": st["step_s"], "cell_updates": st["cell_updates"],
         "with_setup_cell_updates_per_s": st["cell_updates_per_s"],
         "wall_s": st["wall_s"], "batched": batched, "cluster": cl, "concurrency": st["concurrency"],
-        "dc_cycle": cyc, "max_blocks": st["max_blocks"], "batch_loop": a.batch_loop, "batch": st["batch"],
-        "autotune": tune, "clocks": clk}))
+        "dc_cycle": cyc, "max_blocks": st["max_blocks"], "batch_loop": a.batch_loop,
+        "batch": st["batch"], "autotune": tune, "roofline": roof, "clocks": clk}
+
+
+def bench_ensemble(a):
+    import torch
+    r = ensemble_run(a, torch.device("cuda:0"), a.models, a.steps, a.n_max or 128)
+    r.update({"n_gpus": 1, "steps": a.steps, "higher_is_better": True, "dtype": "f32",
+              "data": "synthetic"})
+    print(json.dumps(r))
 
 
 def bench_sloped(a):
@@ -200,34 +249,45 @@ def bench_sloped(a):
         "mass_rel_diff_vs_fp64": mass_rel}))
 
 
-def bench_serving(a):
-    """Poisson arrivals of cubic-grid simulations (log-uniform edge), each
-    a.steps coupled flow/heat/species steps; HBM-budget admission, slots run
-    concurrently; p50/p99 latency and aggregate cell-update rate."""
+def serving_run(a, dev, requests, steps, nmax, rate=20.0, slots=8, clocks=True):
+    """Poisson arrivals of cubic-grid simulations (log-uniform edge 16-nmax),
+    each ``steps`` coupled flow/heat/species steps; HBM-budget admission,
+    state resident on the device, continuous batching of the running
+    requests' solves; p50/p99 latency (arrival to result) and the aggregate
+    cell-update rate over the makespan."""
     import torch
-    set_batch_loop(a)
     from transportse_b200 import workloads
     from transportse_b200.serving import Server, poisson_trace
-    dev = torch.device("cuda:0")
-    nmax = a.n_max or 96
-    trace = poisson_trace(a.requests, a.rate, 5, workloads.serving_request, a.steps, n_min=16,
+    trace = poisson_trace(requests, rate, 5, workloads.serving_request, steps, n_min=16,
                           n_max=nmax)
     budget = min(150e9, torch.cuda.mem_get_info(dev)[0] * 0.85)
-    clocks = ClockSampler(0)
-    clocks.start()
-    reqs, st = Server(device=dev, slots=a.slots, hbm_budget=budget, batched=not a.streams,
-                      cluster=a.cluster, eager=a.gate == "eager").replay(trace)
-    clk = clocks.stop()
-    print(json.dumps({
+    sampler = ClockSampler(0) if clocks else None
+    if sampler:
+        sampler.start()
+    reqs, st = with_loop(Server(device=dev, slots=slots, hbm_budget=budget, batched=not a.streams,
+                                cluster=a.cluster, eager=a.gate == "eager"), a).replay(trace)
+    clk = sampler.stop() if sampler else None
+    peak, peak_kind = measured_peak()
+    roof = batched_roofline(st["cell_updates"], st["batch"], peak, peak_kind)
+    return {
         "metric": "SOR cell-updates/s", "value": st["cell_updates_per_s"], "unit": "cell-updates/s",
-        "n_gpus": 1, "steps": a.steps, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "serving: %d Poisson arrivals at %.0f/s, cubic n log-uniform 16-%d, "
                                "%d steps each, %d slots, HBM budget %.0f GB"
-                               % (a.requests, a.rate, nmax, a.steps, a.slots, budget / 1e9)},
+                               % (requests, rate, nmax, steps, slots, budget / 1e9),
+                   "requests": requests, "steps": steps},
         "latency_p50_s": st["p50_s"], "latency_p99_s": st["p99_s"], "latency_mean_s": st["mean_s"],
-        "makespan_s": st["makespan_s"], "batched": st["batched"], "gate": a.gate,
-        "batch_loop": a.batch_loop,
-        "batch": st["batch"], "clocks": clk}))
+        "makespan_s": st["makespan_s"], "cell_updates": st["cell_updates"],
+        "batched": st["batched"], "gate": a.gate, "batch_loop": a.batch_loop,
+        "batch": st["batch"], "roofline": roof, "clocks": clk}
+
+
+def bench_serving(a):
+    import torch
+    r = serving_run(a, torch.device("cuda:0"), a.requests, a.steps, a.n_max or 96, a.rate,
+                    a.slots)
+    r.update({"n_gpus": 1, "steps": a.steps, "higher_is_better": True, "dtype": "f32",
+              "data": "synthetic"})
+    print(json.dumps(r))
 
 
 def shape_of(a):
@@ -604,6 +664,18 @@ def main():
     if rank == 0 and world == 1 and not a.no_cpu:
         cpu = cpu_pressure_rate(shape, a.cpu_seconds)
     roof = roofline(res, "fp32dc", peak, peak_kind)
+    ens = srv = None
+    if world == 1 and (a.ensemble_models > 0 or a.serving_requests > 0):
+        # the batched form and the serving loop of the same library, after
+        # the single-model state is released
+        del sim
+        torch.cuda.empty_cache()
+        if a.ensemble_models > 0:
+            ens = ensemble_run(a, dev, a.ensemble_models, a.ensemble_steps)
+            torch.cuda.empty_cache()
+        if a.serving_requests > 0:
+            srv = serving_run(a, dev, a.serving_requests, a.serving_steps, a.serving_n_max)
+            torch.cuda.empty_cache()
     if rank == 0:
         print(json.dumps({
             "metric": "SOR cell-updates/s", "value": value, "unit": "cell-updates/s",
@@ -618,7 +690,11 @@ def main():
             # pressure SOR / species / heat separately: each solve call's event
             # time (sweeps, residuals, set-up) and its cell-updates
             "rates_by_solve": res["rates_by_solve"],
-            "roofline": roof, "fp64_plain": fp64, "cpu_baseline": cpu}))
+            "roofline": roof, "fp64_plain": fp64, "cpu_baseline": cpu,
+            # the batched form (the 512-model ensemble of log-uniform 32-128
+            # axes) and the serving loop (Poisson arrivals, p50/p99), measured
+            # in the same run, each with its own roofline and clocks
+            "ensemble": ens, "serving": srv}))
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

@@ -85,7 +85,12 @@ typedef struct TsePressureArgs {
     double *Pn;       /* out: P at entry (the returned Pn) */
     const double *c_f, *nue, *rho_f, *phi, *Kx, *Ky, *Kz, *c_r, *BP, *WP;
     double dt_P, SOR, inc_it, max_dt, min_dt, P_conv;
-    int32_t max_it, reserved;
+    int32_t max_it;
+    int32_t sweep;    /* FP64 solves' sweep kernel for this call (no counterpart
+                         in the reference): 0 the bulk-copy staged kernel
+                         wherever its stages fit, else plain loads (default);
+                         1 plain loads.  Same cell values either way.  The
+                         mixed-precision forms ignore it. */
 } TsePressureArgs;
 
 /* Species transport arguments, compute_C(C, D_fx, D_fy, D_fz, phi, rho_f,
@@ -98,6 +103,8 @@ typedef struct TseSpeciesArgs {
     const double *l_l, *l_t;
     double dt, omega, SOR, inc_it, max_dt, min_dt, conv;
     int32_t max_it, imblflo;
+    int32_t sweep;    /* as TsePressureArgs.sweep */
+    int32_t reserved;
 } TseSpeciesArgs;
 
 /* Heat transport arguments, compute_T(T, l_f, cp_f, rho_f, phi, qx, qy, qz,
@@ -110,6 +117,8 @@ typedef struct TseHeatArgs {
     const double *l_r, *rho_r, *cp_r, *l_l, *l_t;
     double dt, omega, SOR, inc_it, max_dt, min_dt, conv;
     int32_t max_it, imblflo;
+    int32_t sweep;    /* as TsePressureArgs.sweep */
+    int32_t reserved;
 } TseHeatArgs;
 
 /* Workspace kinds for tse_workspace_bytes(). */
@@ -142,11 +151,22 @@ typedef struct TseDcOptions {
     int32_t cycle;            /* in: iterations per correction cycle, <= 0: 256 */
     int32_t max_blocks;       /* in: cap on the sweep kernel's blocks, <= 0: as
                                  many as fit; lets several solves share the GPU */
-    int32_t timing;           /* in: 1 = time the sweep-kernel launches with
-                                 CUDA events on the call's stream */
+    int32_t timing;           /* in: 1 = time the sweep-kernel launches (CUDA
+                                 events on the call's stream; the global timer
+                                 inside the device-driven loop's graph) */
     int32_t sweep_launches;   /* out (timing): sweep-kernel launches */
     int64_t sweep_iterations; /* out (timing): red+black iterations they ran */
     double sweep_ms;          /* out (timing): their summed event time */
+    int32_t host_loop;        /* in, batched fused form only: 0 (default) the
+                                 device-driven loop, one CUDA graph launch per
+                                 call; 1 a host round trip per sweep launch.
+                                 Same results bit for bit. */
+    int32_t reserved;
+    double loop_ms;           /* out (timing, batched fused form): event time of
+                                 the whole loop around the sweeps (plan, sweeps,
+                                 events, x += d, residuals); in the device-driven
+                                 loop sweep_ms is then the sweep kernel's own
+                                 time, taken with the device's global timer */
 } TseDcOptions;
 int32_t tse_compute_P_dc(const TseGrid *grid, const TsePressureArgs *args,
                          TseDcOptions *opts, TseSolveStatus *d_status,
@@ -173,8 +193,13 @@ int32_t tse_compute_T_dc(const TseGrid *grid, const TseHeatArgs *args,
  *   opts->max_blocks <= 0: fused form -- every model's cells in one
  *     cooperative sweep sharing its barriers (models that finish drop out);
  *     the loop around the sweeps runs on the device as one CUDA graph launch
- *     (tse_set_batch_loop: or on the host, one stream synchronisation per
- *     sweep launch); the call returns when every solve is done;
+ *     (a conditional WHILE node whose body plans the launch, sweeps, handles
+ *     each model's events and forms the residuals; the call reads one small
+ *     record at the end) -- or, with opts->host_loop = 1 or on the legacy
+ *     default stream, on the host, one stream synchronisation per sweep
+ *     launch; the same results bit for bit; with opts->timing the device
+ *     loop reports its whole time in sweep_ms; the call returns when every
+ *     solve is done;
  *   opts->max_blocks > 0: cluster form -- one persistent launch with one
  *     thread-block cluster of max_blocks CTAs (at most 16) per model; the
  *     call returns after queueing the work, nothing is read back.
@@ -224,8 +249,10 @@ int32_t tse_compute_T_dc_batch(const TseBatchHeat *items, int32_t n,
  * That holds grids of up to about 43,000 cells (32 x 32 x 32 fits); larger
  * grids return TSE_ERR_WORKSPACE and launch nothing.  The first call on a
  * device looks up the array's device address, so make that first call before
- * any stream capture.  All calls on one GPU share the array: calls that
- * overlap on the GPU (other streams or host threads) race and must be
+ * any stream capture.  The address is kept for the life of the process, so
+ * calls after a cudaDeviceReset (or any teardown of the device's primary
+ * context) are not supported.  All calls on one GPU share the array: calls
+ * that overlap on the GPU (other streams or host threads) race and must be
  * serialised by the caller. */
 #define TSE_NOALLOC_SCRATCH_BYTES (6 * 1024 * 1024)
 int32_t tse_compute_P_noalloc(const TseGrid *grid, const TsePressureArgs *args,
@@ -299,6 +326,27 @@ int32_t tse_eos_linear(const TseGrid *grid, const double *const *h_C,
                        const double *T, double rho0, double tcoef, double T0,
                        double *rho_f, void *stream);
 
+/* Declared per-cell property forms, the GPU form of further callbacks run by
+ * run_fluid_properties (tse.py:179-199), e.g. the temperature polynomials of
+ * course/04-groundwater_heat_tracer_eos/config.py:118-124, 197-219:
+ *   TSE_EOS_CONSTANT  out = coef[0]
+ *   TSE_EOS_POLY4_T   out = coef[4] + coef[3]*T + coef[2]*T**2 + coef[1]*T**3
+ *                           + coef[0]*T**4   (numpy.polyfit order), left to
+ *                     right, with T**3 = T*(T*T) and T**4 = (T*T)*(T*T) as
+ *                     numba computes literal integer powers.
+ * guard (device field or NULL): cells where guard == guard_value keep their
+ * value (the callback's `if C[s] != v:`).  T may be NULL for a constant. */
+#define TSE_EOS_CONSTANT 1
+#define TSE_EOS_POLY4_T 2
+typedef struct TseEosForm {
+  int32_t kind;
+  int32_t reserved;
+  double guard_value;
+  double coef[5];
+} TseEosForm;
+int32_t tse_eos_form(const TseGrid *grid, const TseEosForm *form, const double *T,
+                     const double *guard, double *out, void *stream);
+
 /* Peclet maxima peclet_C / peclet_T (tse.py:331-383), printed diagnostics:
  * d_out[0..2] = max Pe_x, Pe_y, Pe_z over non-boundary cells (NaN
  * propagating; cells on the boundary count as 0 as the zero-initialised
@@ -347,29 +395,8 @@ int32_t tse_mass_totals(const TseGrid *grid, const double *phi,
 int32_t tse_selftest_bounded_waits(int32_t *d_result, double timeout_s, void *d_ws,
                                    size_t ws_bytes, void *stream);
 
-/* Sweep kernel of the FP64 solves (tse_compute_P / _C / _T and the no-alloc
- * pressure solve; no counterpart in the reference): 1 (default) = the staged
- * kernel (bulk asynchronous copies into shared-memory stages, warp-specialized)
- * wherever its stages fit, 0 = plain loads.  Both give the same per-cell
- * values; only the grouping of the convergence check's sums differs.  Applies
- * to calls launched after it, from any host thread.  Returns the previous
- * mode, or TSE_ERR_ARG for a mode other than 0 or 1. */
-int32_t tse_set_exact_sweep(int32_t mode);
-
-/* Loop of the fused batched form (tse_compute_*_dc_batch with max_blocks <= 0;
- * no counterpart in the reference): 1 (default) = device-driven, the whole
- * solve of the batch one CUDA graph launch (a conditional WHILE node whose body
- * plans the launch, sweeps, handles each model's events and forms the
- * residuals on the device; the call reads one small record at the end), 0 = a
- * host loop that reads the models' states after every sweep launch and queues
- * their next steps.  Both give the same results bit for bit; the device-driven
- * loop falls back to the host loop where a graph cannot be built (the legacy
- * default stream).  With opts->timing the device-driven loop reports the whole
- * loop's event time in sweep_ms.  Applies to calls made after it; returns the
- * previous mode, or TSE_ERR_ARG for a mode other than 0 or 1. */
-int32_t tse_set_batch_loop(int32_t mode);
-
-/* Batched solves run so far by the device-driven loop and by the host loop. */
+/* Batched solves run so far by the fused form's device-driven loop and by its
+ * host loop (TseDcOptions.host_loop; no counterpart in the reference). */
 int32_t tse_batch_loop_stats(int64_t *graph_solves, int64_t *host_solves);
 
 /* Library version string. */

@@ -183,6 +183,7 @@ def run(config, max_steps=None, on_step=None, verbose=False, plot_prefix=None):
 
     dt_prev = dt                     # tse.py:1121
     chem = {"inc": 0, "dt_chem": 0}  # tse.py:1132-1133
+    bc_inc = 0                       # tse.py:1128-1132
     dt, dt_prev = plots(t_sim, dt, dt_prev, snapshot)   # tse.py:1177
     while t_sim < t:
         SIA_filled = False
@@ -317,6 +318,19 @@ def run(config, max_steps=None, on_step=None, verbose=False, plot_prefix=None):
         rec = dict(dt=dt, t_sim=t_sim, numitP=numitP, numitC=numitC, numitT=numitT,
                    num_CFL=num_CFL, dt_P=dt_P, dt_C=dt_C, dt_T=dt_T, step=n_tsteps + 1)
         log.append(rec)
+        if config.DYNAMICBC:
+            # tse.py:1448-1458: the hook returns the (possibly replaced) arrays;
+            # a changed bc_inc re-runs the equation of state
+            names = ("P", "T", "C", "BP", "BT", "BC", "WP", "WT", "WC", "Kx", "Ky", "Kz")
+            bc_prev = bc_inc
+            out = config.dynamic_bc(t_sim + dt, bc_inc, *[S[n] for n in names], S["rho_f"],
+                                    S["nue"], S["c_f"], S["cp_f"], S["qx"], S["phi"], S["l_f"],
+                                    S["l_r"])
+            bc_inc = out[0]
+            for n, v in zip(names, out[1:]):
+                S[n] = v
+            if bc_prev != bc_inc and config.FLUIDPROP:
+                update_fluid_properties(config, S)
         if verbose:
             print("[t] %8.2e/%8.2e [dt] %8.2e [S] %4d [P] %3d [C] %3d [T] %3d [CFL] %d"
                   % (t_sim + dt, t, dt, n_tsteps + 1, num_it_P, num_it_C, num_it_T, CFL))

@@ -31,6 +31,65 @@ def config_checksum(cfg):
     return h.hexdigest()
 
 
+def config_attributes(cfg, skip=()):
+    """The array and scalar attributes of a config module, as fixture entries
+    ``cfg_<name>`` (copies: the reference changes its config's arrays in
+    place while it runs)."""
+    out = {}
+    for name in sorted(vars(cfg)):
+        if name.startswith("_") or name in skip:
+            continue
+        v = getattr(cfg, name)
+        if isinstance(v, numpy.ndarray):
+            out["cfg_" + name] = numpy.array(v, copy=True)
+        elif isinstance(v, (bool, int, float, str, numpy.generic)):
+            out["cfg_" + name] = numpy.array(v)
+    return out
+
+
+def course_eos(c_dens, c_visc):
+    """(fluid_properties, GPU_EOS) of the course model with an equation of
+    state, course/04-groundwater_heat_tracer_eos/config.py:197-219: unless
+    species 2 holds 1, density and viscosity are fourth-order polynomials in
+    T with numpy.polyfit coefficients, evaluated left to right with numba's
+    products for literal integer powers (T**3 = T*(T*T), T**4 = (T*T)*(T*T))."""
+    cd = [float(v) for v in c_dens]
+    cv = [float(v) for v in c_visc]
+
+    def fluid_properties(C, T, P, nue, rho_f, c_f, cp_f, l_f, cp_r, l_r, phi, Kx, Ky, Kz,
+                         D_fx, D_fy, D_fz, rho_r):
+        if C[2] != 1:
+            t2 = T * T
+            t3 = T * t2
+            t4 = t2 * t2
+            rho_f = cd[4] + cd[3] * T + cd[2] * t2 + cd[1] * t3 + cd[0] * t4
+            nue = cv[4] + cv[3] * T + cv[2] * t2 + cv[1] * t3 + cv[0] * t4
+        return (C, T, P, nue, rho_f, c_f, cp_f, l_f, cp_r, l_r, phi, Kx, Ky, Kz,
+                D_fx, D_fy, D_fz, rho_r)
+
+    decl = {"rho": {"kind": "poly4_T", "coef": cd, "unless": (2, 1.0)},
+            "nue": {"kind": "poly4_T", "coef": cv, "unless": (2, 1.0)}}
+    return fluid_properties, decl
+
+
+def config_from_fixture(fx, name):
+    """Rebuild a config module from a fixture's ``cfg_<name>`` entries, with
+    the callbacks of the course models (identity EOS and chemistry unless the
+    model declares its own)."""
+    m = types.ModuleType(name)
+    m.__file__ = name + ".py"
+    keys = fx.files if hasattr(fx, "files") else list(fx)
+    for k in keys:
+        if k.startswith("cfg_"):
+            v = numpy.array(fx[k])
+            setattr(m, k[4:], v.item() if v.ndim == 0 else v)
+    m.fluid_properties = workloads._identity_fluid_properties
+    m.chemical_reactions = workloads._noop_chemistry
+    if hasattr(m, "c_dens") and hasattr(m, "c_visc"):
+        m.fluid_properties, m.GPU_EOS = course_eos(m.c_dens, m.c_visc)
+    return m
+
+
 def unit_case(variant):
     """variant 'a': 7x5x6, slope 5 deg, dispersion and IMBLFLO on;
     variant 'b': 6x1x9 slice, no slope, dispersion and IMBLFLO off."""

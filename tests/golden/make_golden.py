@@ -12,7 +12,16 @@ namespace (``exec``), once per synthetic config:
   summary then divides by zero steps, which is caught).
 * end-to-end fixtures (``e2e_*.npz``): a step-counting ``dynamic_bc`` callback
   (tse.py:1448-1458; it returns every field unchanged) records the state after
-  each time step and stops the run after N steps.
+  each time step, a ``mass_balance`` callback (tse.py:1460-1463, called after
+  dynamic_bc and the equation of state it may re-run) records the fields, and
+  the run stops after N steps.  A config with its own ``dynamic_bc`` keeps it:
+  the recorder calls it first.
+* course fixtures (``course_*.npz``): the reference's own example models
+  ``course/01..04/config.py``, loaded from the checkout and run to their end
+  time (PLOTSAVE as configured: the step sequence lands on every PLOTTIME; the
+  snapshot files are counted, not stored).  The fixture holds the config's
+  initial attributes (``cfg_<name>``) so the tests can rebuild it without the
+  checkout, the per-step scalars, and fields at a few steps and at the end.
 
 Usage:  python tests/golden/make_golden.py [--reference PATH] [--only NAME]
 
@@ -85,29 +94,48 @@ SNAPSHOT_ITEMS = ("lx", "ly", "lz", "nx", "ny", "nz", "dx", "dy", "dz", "t_sim",
                   "nue", "cp_f", "l_f", "BP", "BC", "BT", "L", "mass", "WP", "WT", "WC", "e")
 
 
-def run_reference(ref, cfg, steps, keep_steps, fields):
-    """Run ``steps`` time steps; record scalars every step, fields at keep_steps.
-    With PLOTSAVE on, the run happens in a scratch directory and the snapshot
-    files tse.py writes there are recorded item by item ("plot<k>_<item>")."""
+def run_reference(ref, cfg, steps, keep_steps, fields, keep_plots=True):
+    """Run ``steps`` time steps (or to the config's end time, whichever comes
+    first); record scalars every step, fields at keep_steps and at the end
+    ("<field>@final").  With PLOTSAVE on, the run happens in a scratch
+    directory and the snapshot files tse.py writes there are recorded item by
+    item ("plot<k>_<item>"), or only counted ("n_plot_files") without
+    keep_plots."""
     rec = {"dt": [], "t_sim": [], "numitP": [], "numitC": [], "numitT": [],
            "num_CFL": [], "dt_P": [], "dt_C": [], "dt_T": []}
     snaps = {}
+    own_bc = cfg.dynamic_bc if getattr(cfg, "DYNAMICBC", False) else None
+    own_mb = cfg.mass_balance if getattr(cfg, "MASSBALAN", False) else None
     cfg.DYNAMICBC = True
+    cfg.MASSBALAN = True
 
     def dynamic_bc(t, bc_inc, P, T, C, BP, BT, BC, WP, WT, WC, Kx, Ky, Kz, rho_f,
                    nue, c_f, cp_f, qx, phi, l_f, l_r):
         ns = cfg._ns
+        out = (bc_inc, P, T, C, BP, BT, BC, WP, WT, WC, Kx, Ky, Kz)
+        if own_bc is not None:
+            out = own_bc(t, bc_inc, P, T, C, BP, BT, BC, WP, WT, WC, Kx, Ky, Kz, rho_f,
+                         nue, c_f, cp_f, qx, phi, l_f, l_r)
         for k in rec:
             rec[k].append(float(ns.get(k, numpy.nan)))
+        return out
+
+    def mass_balance(C, qx, qy, qz, WP, WC, WT, D_fx, D_fy, D_fz, dt, mass):
+        # called after dynamic_bc and the equation of state it may re-run
+        # (tse.py:1449-1463): the fields here are the step's final ones
+        ns = cfg._ns
+        if own_mb is not None:
+            mass = own_mb(C, qx, qy, qz, WP, WC, WT, D_fx, D_fy, D_fz, dt, mass)
         step = len(rec["dt"])
         if step in keep_steps:
             for f in fields:
                 snaps["%s@%d" % (f, step)] = numpy.array(ns[f], copy=True)
         if step >= steps:
             raise StopRun()
-        return bc_inc, P, T, C, BP, BT, BC, WP, WT, WC, Kx, Ky, Kz
+        return mass
 
     cfg.dynamic_bc = dynamic_bc
+    cfg.mass_balance = mass_balance
     plots = {}
     if getattr(cfg, "PLOTSAVE", False):
         import glob
@@ -119,7 +147,7 @@ def run_reference(ref, cfg, steps, keep_steps, fields):
             try:
                 ns = _exec_reference(ref, cfg)
                 files = sorted(glob.glob("*-[0-9][0-9][0-9][0-9][0-9].p"))
-                for k, f in enumerate(files):
+                for k, f in enumerate(files if keep_plots else ()):
                     for name, v in zip(SNAPSHOT_ITEMS, joblib.load(f)):
                         # later files keep only the items that differ from the
                         # first file's (a missing key means "as in plot0")
@@ -129,9 +157,13 @@ def run_reference(ref, cfg, steps, keep_steps, fields):
                             plots["plot%d_%s" % (k, name)] = v
             finally:
                 os.chdir(cwd)
-        plots["n_plots"] = numpy.array(len(files))
+        plots["n_plots" if keep_plots else "n_plot_files"] = numpy.array(len(files))
     else:
         ns = _exec_reference(ref, cfg)
+    if len(rec["dt"]) < steps:
+        # the run reached the config's end time
+        for f in fields:
+            snaps["%s@final" % f] = numpy.array(ns[f], copy=True)
     out = {("s_" + k): numpy.array(v) for k, v in rec.items()}
     out.update(plots)
     out.update(snaps)
@@ -174,6 +206,8 @@ E2E = {
     "slice_2d_chem": (workloads.slice_2d_chem, {}, 24, {1, 2, 3, 12, 24}, ("P", "C", "phi", "qz")),
     "slice_2d_chemcell": (workloads.slice_2d_chem, {"per_cell": True}, 8, {1, 2, 3, 8},
                           ("P", "C", "phi", "qz")),
+    "slice_2d_dynbc": (workloads.slice_2d_dynbc, {}, 60, {1, 22, 23, 24, 30, 43, 44, 45, 60},
+                       ("P", "C", "qx", "qz", "rho_f", "BC", "BP", "WP")),
 }
 
 
@@ -182,6 +216,39 @@ def gen_e2e(ref, name):
     cfg = builder(**kw)
     data, ns = run_reference(ref, cfg, steps, keep, fields)
     data["config_checksum"] = numpy.array(cases.config_checksum(builder(**kw)))
+    return data
+
+
+COURSE = {
+    # name: (folder under course/, fields, keep_steps) -- run to the end time
+    "course_01": ("01-groundwater_flow", ("P", "qx", "qy"), {1, 10, 100}),
+    "course_02": ("02-groundwater_heat_flow", ("P", "T", "qx", "qy"), {1, 10, 100}),
+    "course_03": ("03-groundwater_heat_tracer_flow", ("P", "T", "C", "qx", "qy"), {1, 10, 100}),
+    "course_04": ("04-groundwater_heat_tracer_eos", ("P", "T", "C", "qx", "qy", "rho_f", "nue"),
+                  {1, 10, 100}),
+}
+# config attributes not stored: the checkout path, the raw EOS table (only
+# its fitted coefficients are used), poly1d objects
+COURSE_SKIP = {"CFDIR", "data"}
+
+
+def load_course_config(ref, folder):
+    import importlib.util
+    path = os.path.join(ref, "course", folder, "config.py")
+    spec = importlib.util.spec_from_file_location("course_" + folder[:2], path)
+    cfg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(cfg)
+    return cfg
+
+
+def gen_course(ref, name):
+    folder, fields, keep = COURSE[name]
+    cfg = load_course_config(ref, folder)
+    data = cases.config_attributes(cfg, skip=COURSE_SKIP)
+    rebuilt = cases.config_from_fixture(data, name)
+    data["config_checksum"] = numpy.array(cases.config_checksum(rebuilt))
+    out, ns = run_reference(ref, cfg, 10 ** 9, keep, fields, keep_plots=False)
+    data.update(out)
     return data
 
 
@@ -212,6 +279,7 @@ def main():
     jobs = [("unit_a", lambda: gen_unit(a.reference, "a")),
             ("unit_b", lambda: gen_unit(a.reference, "b"))]
     jobs += [("e2e_" + n, (lambda n=n: gen_e2e(a.reference, n))) for n in E2E]
+    jobs += [(n, (lambda n=n: gen_course(a.reference, n))) for n in COURSE]
     for name in LOGS:
         if a.only and a.only != "log_" + name:
             continue

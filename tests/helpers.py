@@ -99,3 +99,40 @@ def check_snapshots(files, fx, tol):
                 assert numpy.array_equal(v, ref), (k, name)
             else:
                 assert rel_err(v, ref) <= tol, (k, name, rel_err(v, ref))
+
+
+SCALARS = ("dt", "t_sim", "numitP", "numitC", "numitT", "num_CFL")
+
+
+def run_fixture_case(cfg, fx, device, precision, tmp_path, steps=None):
+    """Run ``cfg`` through the GPU driver the way the fixture ``fx`` was
+    recorded: per-step scalars every step, the fixture's fields at its kept
+    steps (after the step's dynamic_bc and equation of state) and, when the
+    fixture ran to the end time, at the end ("<field>@final").  Returns
+    (scalars, fields, simulation)."""
+    from transportse_b200.driver import Simulation
+    keep = set(int(s) for s in fx["keep_steps"])
+    fields = sorted({k.split("@")[0] for k in fx.files if "@" in k})
+    got = {}
+    scal = {k: [] for k in SCALARS}
+
+    def tap(rec, sim):
+        for k in scal:
+            scal[k].append(rec[k])
+        if rec["step"] in keep:
+            for f in fields:
+                got["%s@%d" % (f, rec["step"])] = sim.field(f)
+
+    sim = Simulation(cfg, device=device, precision=precision, plot_prefix=str(tmp_path / "snap"))
+    sim.run(max_steps=steps, on_step=tap)
+    if any(k.endswith("@final") for k in fx.files):
+        for f in fields:
+            got[f + "@final"] = sim.field(f)
+    return scal, got, sim
+
+
+def dynamic_pressure_err(got_P, ref_P, P0):
+    """The pressure change since the start (P - P0, mostly the flow-driven
+    part: P itself is dominated by the hydrostatic head) compared on its own
+    scale."""
+    return rel_err(numpy.asarray(got_P) - P0, numpy.asarray(ref_P) - P0)

@@ -109,31 +109,24 @@ def test_selftest_validates_without_gpu():
     assert L.tse_selftest_bounded_waits(ct.c_void_p(16), 0.0, ct.c_void_p(4096), 512, None) == -1
 
 
-def test_exact_sweep_mode_switch_without_gpu():
-    """The FP64 sweep selector takes 0 or 1, returns the previous mode and
-    refuses anything else (no device call)."""
+def test_per_call_selectors_match_the_header_layout():
+    """The sweep and loop selectors are fields of each call's structs (no
+    process-wide switch): their offsets follow the header's layout."""
+    assert N.TsePressureArgs.sweep.offset == 12 * 8 + 6 * 8 + 4
+    assert ct.sizeof(N.TsePressureArgs) == 12 * 8 + 6 * 8 + 8
+    for T, nptr in ((N.TseSpeciesArgs, 15), (N.TseHeatArgs, 16)):
+        assert T.sweep.offset == nptr * 8 + 7 * 8 + 8
+        assert ct.sizeof(T) == nptr * 8 + 7 * 8 + 16
+    assert N.TseDcOptions.host_loop.offset == 32 and N.TseDcOptions.loop_ms.offset == 40
+    assert ct.sizeof(N.TseDcOptions) == 48
     L = N.lib()
-    prev = L.tse_set_exact_sweep(0)
-    try:
-        assert prev in (0, 1)
-        assert L.tse_set_exact_sweep(1) == 0
-        assert L.tse_set_exact_sweep(1) == 1
-        assert L.tse_set_exact_sweep(2) == -1 and L.tse_set_exact_sweep(-1) == -1
-    finally:
-        L.tse_set_exact_sweep(prev)
+    for name in ("tse_set_exact_sweep", "tse_set_batch_loop"):
+        assert not hasattr(L, name)
 
 
-def test_batch_loop_switch_and_stats_without_gpu():
-    """The batched form's loop selector takes 0 or 1 and returns the previous
-    mode; the loop statistics read without a device call."""
+def test_batch_loop_stats_without_gpu():
+    """The batched form's loop statistics read without a device call."""
     L = N.lib()
-    prev = L.tse_set_batch_loop(0)
-    try:
-        assert prev in (0, 1)
-        assert L.tse_set_batch_loop(1) == 0
-        assert L.tse_set_batch_loop(3) == -1
-    finally:
-        L.tse_set_batch_loop(prev)
     g, h = ct.c_int64(-1), ct.c_int64(-1)
     assert L.tse_batch_loop_stats(ct.byref(g), ct.byref(h)) == 0
     assert g.value >= 0 and h.value >= 0

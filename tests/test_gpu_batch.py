@@ -16,11 +16,11 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-6
 
 
-def _run_members(fns, device, cluster=0):
+def _run_members(fns, device, cluster=0, host_loop=False):
     """Run fns[i](gate) on threads of their own, each on its own stream, all
     joined to one gate before any starts (so the first solves batch)."""
     from transportse_b200.batch import BatchGate
-    gate = BatchGate(device, cluster=cluster)
+    gate = BatchGate(device, cluster=cluster, host_loop=host_loop)
     out = [None] * len(fns)
     errs = []
     for _ in fns:
@@ -129,18 +129,15 @@ def test_device_loop_equals_host_loop(kw, cuda_device):
         return fn
 
     out, used = {}, {}
-    prev = lib.tse_set_batch_loop(1)
-    try:
-        for mode in (1, 0):
-            lib.tse_set_batch_loop(mode)
-            g0, h0 = ct.c_int64(), ct.c_int64()
-            lib.tse_batch_loop_stats(ct.byref(g0), ct.byref(h0))
-            out[mode], _ = _run_members([member(i) for i in range(len(SHAPES))], cuda_device)
-            g1, h1 = ct.c_int64(), ct.c_int64()
-            lib.tse_batch_loop_stats(ct.byref(g1), ct.byref(h1))
-            used[mode] = (g1.value - g0.value, h1.value - h0.value)
-    finally:
-        lib.tse_set_batch_loop(prev)
+    for mode in (1, 0):
+        g0, h0 = ct.c_int64(), ct.c_int64()
+        lib.tse_batch_loop_stats(ct.byref(g0), ct.byref(h0))
+        # per call: TseDcOptions.host_loop = 0 device-driven, 1 host loop
+        out[mode], _ = _run_members([member(i) for i in range(len(SHAPES))], cuda_device,
+                                    host_loop=mode == 0)
+        g1, h1 = ct.c_int64(), ct.c_int64()
+        lib.tse_batch_loop_stats(ct.byref(g1), ct.byref(h1))
+        used[mode] = (g1.value - g0.value, h1.value - h0.value)
     assert used[1] == (1, 0) and used[0] == (0, 1), used
     for i, (a, b) in enumerate(zip(out[1], out[0])):
         assert (a[0], a[1], a[4], a[5]) == (b[0], b[1], b[4], b[5]), SHAPES[i]

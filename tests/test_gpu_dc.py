@@ -2,17 +2,21 @@
 reference: the golden unit fixtures (outputs of tse.py's numba kernels), the
 oracle on further shapes, and the reference's end-to-end runs.
 
-Tolerance: 1e-6 relative to each field's scale (the FP32+refinement bound);
-convergence flags and the dt sequence must match; iteration counts may differ
-by a few check intervals because the change of the FP32 correction is
-measured in FP32."""
+Tolerance: 1e-6 relative to each field's scale (the FP32+refinement bound),
+for every field the fixtures hold -- pressure, concentrations, temperature,
+the Darcy fluxes it drives, density -- and for the pressure change since the
+start (P - P0) on its own scale, so the flow-driven part of the pressure is
+not hidden under the hydrostatic head; convergence flags and the dt sequence
+must match; iteration counts may differ by a few check intervals because the
+change of the FP32 correction is measured in FP32."""
 import numpy
 import pytest
 
 from oracle.oracle import OracleModel
 from tests.golden import cases
-from tests.golden.make_golden import E2E
-from tests.helpers import NumpyKernels, check_snapshots, load, model_for, rel_err
+from tests.golden.make_golden import COURSE, E2E
+from tests.helpers import (NumpyKernels, check_snapshots, dynamic_pressure_err, load, model_for,
+                           rel_err, run_fixture_case)
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-6
@@ -92,7 +96,29 @@ def test_dc_driver_matches_reference_run(name, cuda_device, tmp_path):
     sim.run(max_steps=steps, on_step=tap)
     if "n_plots" in fx.files:
         check_snapshots(sim.plots.written, fx, TOL)
+    P0 = numpy.asarray(cfg.P)
     for k in fx.files:
-        if "@" in k and k.split("@")[0] in ("P", "C", "T"):
+        if "@" in k:
             e = rel_err(got[k], fx[k])
             assert e <= TOL, (k, e)
+            if k.startswith("P@"):
+                assert dynamic_pressure_err(got[k], fx[k], P0) <= TOL, k
+
+
+@pytest.mark.parametrize("name", sorted(COURSE))
+def test_dc_driver_matches_reference_course_models(name, cuda_device, tmp_path):
+    """The reference's example models (course/01..04) to their end time in the
+    mixed-precision form: every field and the pressure change within 1e-6, the
+    step count and snapshot count equal, the time within 1e-6 at every step."""
+    fx = load(name)
+    cfg = cases.config_from_fixture(fx, name)
+    scal, got, sim = run_fixture_case(cfg, fx, cuda_device, "fp32dc", tmp_path)
+    assert len(scal["dt"]) == len(fx["s_dt"])
+    assert len(sim.plots.written) == int(fx["n_plot_files"])
+    assert rel_err(numpy.array(scal["t_sim"]), fx["s_t_sim"]) <= TOL
+    P0 = numpy.asarray(cfg.P)
+    for k in fx.files:
+        if "@" in k:
+            assert rel_err(got[k], fx[k]) <= TOL, (k, rel_err(got[k], fx[k]))
+            if k.startswith("P@"):
+                assert dynamic_pressure_err(got[k], fx[k], P0) <= TOL, k

@@ -6,8 +6,9 @@ import numpy
 import pytest
 
 from tests.golden import cases
-from tests.golden.make_golden import E2E
-from tests.helpers import check_snapshots, load, rel_err
+from tests.golden.make_golden import COURSE, E2E
+from tests.helpers import (check_snapshots, dynamic_pressure_err, load, rel_err,
+                           run_fixture_case)
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-9
@@ -44,3 +45,27 @@ def test_driver_matches_reference_run(name, cuda_device, tmp_path):
             e = rel_err(got[k], fx[k])
             worst = max(worst, e)
             assert e <= TOL, (k, e)
+
+
+@pytest.mark.parametrize("name", sorted(COURSE))
+def test_driver_matches_reference_course_models(name, cuda_device, tmp_path):
+    """The reference's own example models (course/01..04: flow; heat; heat and
+    tracer; the polynomial EOS declared for the device), run to their end time
+    (649-852 steps, snapshot times landed on): every step's dt and t within
+    1e-9 and its iteration counts exact, fields within 1e-9, the snapshot
+    count equal."""
+    fx = load(name)
+    cfg = cases.config_from_fixture(fx, name)
+    assert cases.config_checksum(cfg) == str(fx["config_checksum"])
+    scal, got, sim = run_fixture_case(cfg, fx, cuda_device, "fp64", tmp_path)
+    assert len(sim.plots.written) == int(fx["n_plot_files"])
+    for k in ("numitP", "numitC", "numitT", "num_CFL"):
+        assert numpy.array_equal(numpy.array(scal[k]), fx["s_" + k]), k
+    for k in ("dt", "t_sim"):
+        assert rel_err(numpy.array(scal[k]), fx["s_" + k]) <= TOL, k
+    P0 = numpy.asarray(cfg.P)
+    for k in fx.files:
+        if "@" in k:
+            assert rel_err(got[k], fx[k]) <= TOL, (k, rel_err(got[k], fx[k]))
+            if k.startswith("P@"):
+                assert dynamic_pressure_err(got[k], fx[k], P0) <= TOL, k

@@ -182,22 +182,48 @@ def test_staged_and_plain_exact_solves_agree(shape, cuda_device):
     m = model_for(cfg, cuda_device)
     nk = NumpyKernels(m)
     out = {}
-    prev = lib.tse_set_exact_sweep(1)
-    try:
-        for mode in (1, 0):
-            assert lib.tse_set_exact_sweep(mode) in (0, 1)
-            rp = nk.compute_P(P.copy(), f["c_f"], f["nue"], f["rho_f"], f["phi"], K, K * 0.7, K * 0.2,
-                              z, z, z, 3600.0, BP, WP, SOR=1.7, max_it=20000, inc_it=1.25,
-                              max_dt=1e5, min_dt=1e-8, P_conv=1e-10)
-            rc = [nk.compute_C(C.copy(), D, D, D, f["phi"], f["rho_f"], *q, 3600.0, BC, WC,
-                               numpy.ones(shp), e, omega=om, SOR=1.1, max_it=100, inc_it=1.05,
-                               max_dt=1e5, min_dt=1e-8, C_conv=1e-12) for om in (1, 0.5)]
-            out[mode] = (rp, rc)
-    finally:
-        lib.tse_set_exact_sweep(prev)
-    (p1, c1), (p0, c0) = out[1], out[0]
+    for mode in (0, 1):
+        m.sweep = mode   # per call: 0 staged bulk-copy kernel, 1 plain loads
+        rp = nk.compute_P(P.copy(), f["c_f"], f["nue"], f["rho_f"], f["phi"], K, K * 0.7, K * 0.2,
+                          z, z, z, 3600.0, BP, WP, SOR=1.7, max_it=20000, inc_it=1.25,
+                          max_dt=1e5, min_dt=1e-8, P_conv=1e-10)
+        rc = [nk.compute_C(C.copy(), D, D, D, f["phi"], f["rho_f"], *q, 3600.0, BC, WC,
+                           numpy.ones(shp), e, omega=om, SOR=1.1, max_it=100, inc_it=1.05,
+                           max_dt=1e5, min_dt=1e-8, C_conv=1e-12) for om in (1, 0.5)]
+        out[mode] = (rp, rc)
+    (p1, c1), (p0, c0) = out[0], out[1]
     assert p1[5] > 20 and (p1[0], p1[1], p1[4], p1[5]) == (p0[0], p0[1], p0[4], p0[5])
     assert numpy.array_equal(p1[2], p0[2])
     for a, b in zip(c1, c0):
         assert (a[0], a[1], a[3], a[4]) == (b[0], b[1], b[3], b[4])
         assert numpy.array_equal(a[2], b[2])
+
+
+def test_declared_eos_forms_bit_exact(cuda_device):
+    """tse_eos_form (constant; fourth-order polynomial in T, guarded by a
+    species) against the host evaluation the declaration is validated with,
+    bit for bit, including the guarded cells, which keep their value."""
+    import torch
+    from transportse_b200 import eos, workloads
+    cfg = workloads.base_config("eos", 17, 5, 9, 1.0, 1.0, 1.0, species=3)
+    m = model_for(cfg, cuda_device)
+    rng = numpy.random.default_rng(12)
+    shp = (17, 5, 9)
+    T = rng.uniform(-5.0, 160.0, shp)
+    guard = numpy.where(rng.uniform(size=shp) < 0.3, 1.0, rng.uniform(0, 2, shp))
+    old = rng.uniform(900.0, 1100.0, shp)
+    coef = [2.1e-8, -7.3e-6, -3.7e-3, 0.05, 999.8]
+    forms = [{"kind": "poly4_T", "coef": coef, "unless": (2, 1.0)},
+             {"kind": "poly4_T", "coef": coef},
+             {"kind": "constant", "value": 1.234e-3, "unless": (2, 1.0)}]
+    dev = lambda a: torch.as_tensor(a, device=cuda_device)
+    for d in forms:
+        out = dev(old.copy())
+        g = dev(guard) if "unless" in d else None
+        m.eos_form(d["kind"], d.get("coef", d.get("value")), dev(T), out, g,
+                   d.get("unless", (0, 0.0))[1])
+        got = out.cpu().numpy()
+        want = numpy.empty(shp)
+        for c in numpy.ndindex(shp):
+            want[c] = eos.eval_form_host(d, [0.0, 0.0, guard[c]], T[c], old[c])
+        assert numpy.array_equal(got, want), d

@@ -62,6 +62,56 @@ def test_declared_eos_validates_against_callback():
         eos.validate(cfg, bad)
 
 
+def test_declared_polynomial_eos_of_the_course_model_validates():
+    """The course model with an equation of state (course/04): density and
+    viscosity polynomials in T, guarded by species 2.  The declaration matches
+    the callback bit for bit (the probes include C[2] == 1, the guarded case);
+    a changed coefficient, a changed guard or plain pow() powers do not."""
+    from tests.golden import cases
+    from tests.helpers import load
+    cfg = cases.config_from_fixture(load("course_04"), "course_04")
+    decl = eos.declared_eos(cfg)
+    assert decl["rho"]["kind"] == "poly4_T" and decl["nue"]["unless"] == (2, 1.0)
+    assert eos.validate(cfg, decl)
+    bad = dict(decl, nue=dict(decl["nue"], coef=[v * (1 + 1e-12) for v in decl["nue"]["coef"]]))
+    with pytest.raises(eos.EOSMismatch):
+        eos.validate(cfg, bad)
+    with pytest.raises(eos.EOSMismatch):
+        eos.validate(cfg, dict(decl, rho=dict(decl["rho"], unless=(1, 1.0))))
+    cd = [float(v) for v in cfg.c_dens]
+
+    def pow_callback(C, T, P, nue, rho_f, *rest):
+        if C[2] != 1:
+            rho_f = cd[4] + cd[3] * T + cd[2] * T ** 2 + cd[1] * T ** 3 + cd[0] * T ** 4
+        return (C, T, P, nue, rho_f) + rest
+
+    # the same polynomial through libm's pow differs in the last bit somewhere
+    T = numpy.random.default_rng(3).uniform(0.0, 150.0, 4000)
+    rho = {"kind": "poly4_T", "coef": cd}
+    assert any(eos.eval_form_host(rho, [0, 0, 0], t, 0.0) != pow_callback(
+        [0, 0, 0], t, 0, 0, 0)[4] for t in T)
+
+
+def test_declared_eos_forms_are_checked():
+    cfg = workloads.slice_2d(6, 1, 4)
+    cfg.GPU_EOS = {"rho": {"kind": "poly4_T", "coef": [1, 2, 3]}}
+    with pytest.raises(ValueError):
+        eos.declared_eos(cfg)
+    cfg.GPU_EOS = {"nue": {"kind": "linear"}}
+    with pytest.raises(ValueError):
+        eos.declared_eos(cfg)
+    cfg.GPU_EOS = {"rho": {"kind": "linear", "rho0": 1000.0, "species": [], "tcoef": 0.0,
+                           "T0": 0.0, "unless": (0, 1.0)}}
+    with pytest.raises(ValueError):
+        eos.declared_eos(cfg)
+    cfg.GPU_EOS = {"visc": {"kind": "keep"}}
+    with pytest.raises(ValueError):
+        eos.declared_eos(cfg)
+    cfg.GPU_EOS = {"nue": {"kind": "constant", "value": 1e-3}}
+    d = eos.declared_eos(cfg)
+    assert d["rho"]["kind"] == "keep" and d["nue"]["value"] == 1e-3
+
+
 def test_hbm_budget_blocks_until_release():
     from transportse_b200.ensemble import HbmBudget
     b = HbmBudget(100)

@@ -7,7 +7,7 @@ import pytest
 from oracle import driver as odriver
 from oracle.oracle import OracleModel
 from tests.golden import cases
-from tests.golden.make_golden import E2E
+from tests.golden.make_golden import COURSE, E2E
 from tests.helpers import check_snapshots, load
 
 
@@ -44,6 +44,37 @@ def test_oracle_driver_bit_exact(name, tmp_path):
     S = odriver.run(cfg, max_steps=steps, on_step=tap, plot_prefix=str(tmp_path / "snap"))
     if "n_plots" in fx.files:
         check_snapshots(S["plots"], fx, 0)
+    for k, v in scal.items():
+        assert numpy.array_equal(numpy.array(v), fx["s_" + k]), k
+    for k in fx.files:
+        if "@" in k:
+            assert numpy.array_equal(fx[k], got[k]), k
+
+
+@pytest.mark.parametrize("name", sorted(COURSE))
+def test_oracle_course_models_bit_exact(name, tmp_path):
+    """The reference's own example models (course/01..04), run to their end
+    time with snapshots on: every step's dt, t and iteration counts, the fields
+    at the kept steps and at the end, and the number of snapshot files."""
+    fx = load(name)
+    cfg = cases.config_from_fixture(fx, name)
+    assert cases.config_checksum(cfg) == str(fx["config_checksum"])
+    keep = set(int(s) for s in fx["keep_steps"])
+    fields = sorted({k.split("@")[0] for k in fx.files if "@" in k})
+    got = {}
+    scal = {k: [] for k in ("dt", "t_sim", "numitP", "numitC", "numitT", "num_CFL")}
+
+    def tap(rec, S):
+        for k in scal:
+            scal[k].append(rec[k])
+        if rec["step"] in keep:
+            for f in fields:
+                got["%s@%d" % (f, rec["step"])] = S[f].copy()
+
+    S = odriver.run(cfg, on_step=tap, plot_prefix=str(tmp_path / "snap"))
+    for f in fields:
+        got[f + "@final"] = S[f]
+    assert len(S["plots"]) == int(fx["n_plot_files"])
     for k, v in scal.items():
         assert numpy.array_equal(numpy.array(v), fx["s_" + k]), k
     for k in fx.files:

@@ -96,6 +96,9 @@ def test_noalloc_matches_workspace_solve_twice(cuda_device):
         assert s_new.t == s_ref.t and s_new.dt == s_ref.dt, call
         assert _rel(P_new, P_ref) <= TOL, call
         assert _rel(Pn_new, Pn_ref) <= TOL, call
+        # the same kernels on the same inputs: equal bit for bit, which would
+        # also show anything left over in the shared scratch
+        assert torch.equal(P_new, P_ref) and torch.equal(Pn_new, Pn_ref), call
         dt_ref, dt_new = s_ref.dt, s_new.dt
 
 

@@ -47,27 +47,39 @@ class TsePressureArgs(ct.Structure):
     _fields_ = _ptr_fields(["P", "Pn", "c_f", "nue", "rho_f", "phi", "Kx", "Ky", "Kz", "c_r",
                             "BP", "WP"]) + \
         [(n, ct.c_double) for n in ("dt_P", "SOR", "inc_it", "max_dt", "min_dt", "P_conv")] + \
-        [("max_it", ct.c_int32), ("reserved", ct.c_int32)]
+        [("max_it", ct.c_int32), ("sweep", ct.c_int32)]
 
 
 class TseSpeciesArgs(ct.Structure):
     _fields_ = _ptr_fields(["C", "D_fx", "D_fy", "D_fz", "phi", "rho_f", "qx", "qy", "qz", "BC",
                             "WC", "RC", "e", "l_l", "l_t"]) + \
         [(n, ct.c_double) for n in ("dt", "omega", "SOR", "inc_it", "max_dt", "min_dt", "conv")] + \
-        [("max_it", ct.c_int32), ("imblflo", ct.c_int32)]
+        [("max_it", ct.c_int32), ("imblflo", ct.c_int32), ("sweep", ct.c_int32),
+         ("reserved", ct.c_int32)]
 
 
 class TseHeatArgs(ct.Structure):
     _fields_ = _ptr_fields(["T", "l_f", "cp_f", "rho_f", "phi", "qx", "qy", "qz", "BT", "WT", "e",
                             "l_r", "rho_r", "cp_r", "l_l", "l_t"]) + \
         [(n, ct.c_double) for n in ("dt", "omega", "SOR", "inc_it", "max_dt", "min_dt", "conv")] + \
-        [("max_it", ct.c_int32), ("imblflo", ct.c_int32)]
+        [("max_it", ct.c_int32), ("imblflo", ct.c_int32), ("sweep", ct.c_int32),
+         ("reserved", ct.c_int32)]
+
+
+TSE_EOS_CONSTANT = 1
+TSE_EOS_POLY4_T = 2
+
+
+class TseEosForm(ct.Structure):
+    _fields_ = [("kind", ct.c_int32), ("reserved", ct.c_int32), ("guard_value", ct.c_double),
+                ("coef", ct.c_double * 5)]
 
 
 class TseDcOptions(ct.Structure):
     _fields_ = [("cycle", ct.c_int32), ("max_blocks", ct.c_int32), ("timing", ct.c_int32),
                 ("sweep_launches", ct.c_int32), ("sweep_iterations", ct.c_int64),
-                ("sweep_ms", ct.c_double)]
+                ("sweep_ms", ct.c_double), ("host_loop", ct.c_int32), ("reserved", ct.c_int32),
+                ("loop_ms", ct.c_double)]
 
 
 def _batch_item(args_type):
@@ -119,13 +131,12 @@ SIGNATURES = {
     "tse_explicit_C": (_I, [_G, _PP, _I, _P, _P, _P, _S, _P]),
     "tse_field_stats": (_I, [_P, ct.c_int64, _P, _P, _S, _P]),
     "tse_eos_linear": (_I, [_G, _PP, ct.POINTER(ct.c_int32), _dp, _I, _P, _D, _D, _D, _P, _P]),
+    "tse_eos_form": (_I, [_G, ct.POINTER(TseEosForm), _P, _P, _P, _P]),
     "tse_peclet_C": (_I, [_G, _P, _P, _P, _PP, _PP, _PP, _I, _P, _P, _P, _S, _P]),
     "tse_peclet_T": (_I, [_G, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, _S, _P]),
     "tse_mass_totals": (_I, [_G, _P, _P, _P, _PP, _PP, _I, _P, _P, _P, _P, _P, _P, _P, _P, _S,
                              _P]),
     "tse_selftest_bounded_waits": (_I, [_P, _D, _P, _S, _P]),
-    "tse_set_exact_sweep": (_I, [_I]),
-    "tse_set_batch_loop": (_I, [_I]),
     "tse_batch_loop_stats": (_I, [ct.POINTER(ct.c_int64), ct.POINTER(ct.c_int64)]),
     "tse_version": (ct.c_char_p, []),
 }

@@ -23,6 +23,7 @@ from __future__ import annotations
 
 import ctypes as ct
 import threading
+import time
 from contextlib import contextmanager
 
 import torch
@@ -62,13 +63,18 @@ class BatchGate:
     the gate's lock is free while a batch runs, and a model's results do not
     depend on which batch it was in.
 
+    ``host_loop``: the fused form's loop around its sweep launches -- False
+    (default) on the device, one CUDA graph launch per batched call; True on
+    the host, a round trip per sweep launch.  Same results bit for bit.
+
     Use ``with gate.member():`` around a member thread's work, and attach the
     gate to its model (``Model.batch_gate = gate``)."""
 
-    def __init__(self, device=None, cluster=0, eager=False):
+    def __init__(self, device=None, cluster=0, eager=False, host_loop=False):
         self.device = torch.device(device if device is not None else "cuda")
         self.cluster = int(cluster)
         self.eager = bool(eager)
+        self.host_loop = bool(host_loop)
         self.cv = threading.Condition(threading.Lock())
         self.members = 0
         self.running = 0
@@ -79,8 +85,14 @@ class BatchGate:
         # statistics: launches per kind and models per launch
         self.launches = {k: 0 for k in KINDS}
         self.solves = {k: 0 for k in KINDS}
-        # fused form: sweep launches, global iterations, event ms per kind
-        self.sweeps = {k: [0, 0, 0.0] for k in KINDS}
+        # fused form: sweep launches, global iterations, sweep ms and loop ms per kind
+        self.sweeps = {k: [0, 0, 0.0, 0.0] for k in KINDS}
+        # host wall time inside the batched calls, and between the end of one
+        # batch and the issue of the next (the members' host work while no
+        # batch runs)
+        self.call_s = 0.0
+        self.gap_s = 0.0
+        self._t_end = None
 
     # ------------------------------------------------------- membership
     def join(self):
@@ -133,13 +145,19 @@ class BatchGate:
             self.launching = True
             self.cv.release()
             err = None
+            t0 = time.perf_counter()
             try:
                 self._launch(reqs)
             except Exception as e:   # every waiting member sees the failure
                 err = e
             finally:
+                t1 = time.perf_counter()
                 self.cv.acquire()
                 self.launching = False
+                if self._t_end is not None and not self.eager:
+                    self.gap_s += max(0.0, t0 - self._t_end)
+                self.call_s += t1 - t0
+                self._t_end = t1
             for r in reqs:
                 r.error = err
                 r.done = True
@@ -181,6 +199,7 @@ class BatchGate:
                                                 ct.c_void_p(r.ws.data_ptr()), r.ws_bytes)
                                            for r in rs])
                 opts = N.TseDcOptions(cycle, self.cluster, 1)
+                opts.host_loop = int(self.host_loop)
                 rc = getattr(L, "tse_%s_dc_batch" % name)(items, len(rs), ct.byref(opts),
                                                           ct.c_void_p(ws.data_ptr()), ws.numel(),
                                                           ct.c_void_p(bs.cuda_stream))
@@ -190,10 +209,16 @@ class BatchGate:
                 self.sweeps[name][0] += opts.sweep_launches
                 self.sweeps[name][1] += opts.sweep_iterations
                 self.sweeps[name][2] += opts.sweep_ms
+                self.sweeps[name][3] += opts.loop_ms
                 for r in rs:
                     r.stream.wait_stream(bs)
 
     def stats(self):
+        # sweeps: the fused sweep kernel's launches, the global iterations
+        # they ran and their own time (ms); loop_ms: the whole loop around
+        # them (sweeps, events, x += d, residuals)
         return {"launches": dict(self.launches), "solves": dict(self.solves),
-                "sweeps": {k: {"launches": v[0], "iterations": v[1], "ms": round(v[2], 3)}
+                "call_s": round(self.call_s, 3), "gap_s": round(self.gap_s, 3),
+                "sweeps": {k: {"launches": v[0], "iterations": v[1], "ms": round(v[2], 3),
+                               "loop_ms": round(v[3], 3)}
                            for k, v in self.sweeps.items()}}

@@ -28,6 +28,7 @@
 #include <vector>
 #include <algorithm>
 #include <atomic>
+#include <chrono>
 #include <cooperative_groups.h>
 
 #include "tse_dc.cuh"
@@ -614,13 +615,22 @@ __global__ void __launch_bounds__(kTmaConsumers + 32 * PIPES, PIPES == 1 ? 2 : 1
     fused_sweep_body<RING, PIPES>(A, T);
 }
 
+struct FusedCtl;
+__device__ void fused_add_sweep_ns(FusedCtl* ctl, unsigned long long ns);
+
 // the same with its arguments in device memory, written by the plan kernel
-// of the device-driven loop
+// of the device-driven loop; block 0 adds the launch's duration (global
+// timer, from its start to after the launch's last device-wide barrier) to
+// the loop's sweep time, the kernel's own time inside the graph, where no
+// host event can bracket it
 template <int RING, int PIPES>
 __global__ void __launch_bounds__(kTmaConsumers + 32 * PIPES, PIPES == 1 ? 2 : 1)
-    fused_sweep_dev_kernel(const FusedArgs* Ad, TmaStage T) {
+    fused_sweep_dev_kernel(const FusedArgs* Ad, TmaStage T, FusedCtl* ctl) {
+    const bool clock = blockIdx.x == 0 && threadIdx.x == 0;
+    const uint64_t t0 = clock ? globaltimer() : 0;
     const FusedArgs A = *Ad;
     fused_sweep_body<RING, PIPES>(A, T);
+    if (clock) fused_add_sweep_ns(ctl, globaltimer() - t0);
 }
 
 __global__ void fused_gather_kernel(const FusedItem* items, int n, DcState* out) {
@@ -722,9 +732,12 @@ static int run_fused(std::vector<BatchItem<Form>>& v, TseDcOptions* opts, void* 
         opts->sweep_launches = 0;
         opts->sweep_iterations = 0;
         opts->sweep_ms = 0.0;
+        opts->loop_ms = 0.0;
         if (cudaEventCreate(&ev0) != cudaSuccess || cudaEventCreate(&ev1) != cudaSuccess)
             return TSE_ERR_LAUNCH;
     }
+    // the host loop synchronises every launch: its wall time is the loop's
+    const auto loop_t0 = std::chrono::steady_clock::now();
     std::vector<FusedItem> hitems;
     std::vector<FusedChunk> hchunks;
     std::vector<DcState> got;
@@ -844,6 +857,8 @@ static int run_fused(std::vector<BatchItem<Form>>& v, TseDcOptions* opts, void* 
         active.swap(next);
     }
     if (timing) {
+        opts->loop_ms =
+            std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - loop_t0).count();
         cudaEventDestroy(ev0);
         cudaEventDestroy(ev1);
     }
@@ -880,7 +895,10 @@ struct FusedCtl {
     int launches;            // sweep launches over the whole solve
     long long iterations;    // global iterations over the whole solve
     long long resid_total;   // residual blocks of the current body run, all models
+    unsigned long long sweep_ns;   // summed duration of the sweep launches
 };
+
+__device__ void fused_add_sweep_ns(FusedCtl* ctl, unsigned long long ns) { ctl->sweep_ns += ns; }
 
 // one model of the device-driven loop
 struct FusedModel {
@@ -1157,9 +1175,6 @@ static size_t fused_loop_bytes(int n) {
            align256(sizeof(FusedArgs)) + align256(sizeof(FusedCtl)) + align256(form * n);
 }
 
-// 1: the device-driven loop (default); 0: run_fused's host loop
-int batch_loop_mode();
-
 // batch solves run by each loop since the library was loaded
 std::atomic<long long> g_graph_solves{0}, g_host_solves{0};
 
@@ -1169,7 +1184,7 @@ std::atomic<long long> g_graph_solves{0}, g_host_solves{0};
 template <class Form>
 static int run_fused_graph(std::vector<BatchItem<Form>>& v, TseDcOptions* opts, void* d_ws, size_t ws_bytes,
                            cudaStream_t stream) {
-    if (batch_loop_mode() != 1 || stream == nullptr) return 1;
+    if ((opts && opts->host_loop == 1) || stream == nullptr) return 1;
     const int n = (int)v.size();
     long long cells = 0;
     int Hmax = 0;
@@ -1266,7 +1281,8 @@ static int run_fused_graph(std::vector<BatchItem<Form>>& v, TseDcOptions* opts, 
         lc.attrs = at;
         lc.numAttrs = 1;
         const FusedArgs* a_ptr = d_args;
-        void* kargs[] = {(void*)&a_ptr, (void*)&T};
+        FusedCtl* c_ptr = d_ctl;
+        void* kargs[] = {(void*)&a_ptr, (void*)&T, (void*)&c_ptr};
         const cudaError_t le = cudaLaunchKernelExC(&lc, kernel, kargs);
         fused_events_kernel<<<1, kPlanThreads, 0, stream>>>(d_ctl, d_models, d_args, d_idx, d_act, d_rstart,
                                                             cond);
@@ -1343,7 +1359,8 @@ static int run_fused_graph(std::vector<BatchItem<Form>>& v, TseDcOptions* opts, 
         cudaEventElapsedTime(&ms, ev0, ev1);
         opts->sweep_launches = hc.launches;
         opts->sweep_iterations = hc.iterations;
-        opts->sweep_ms = ms;
+        opts->sweep_ms = (double)hc.sweep_ns * 1e-6;
+        opts->loop_ms = ms;
         cudaEventDestroy(ev0);
         cudaEventDestroy(ev1);
     }

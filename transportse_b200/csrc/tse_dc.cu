@@ -654,6 +654,7 @@ static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, 
         opts->sweep_launches = 0;
         opts->sweep_iterations = 0;
         opts->sweep_ms = 0.0;
+        opts->loop_ms = 0.0;
         if (cudaEventCreate(&ev0) != cudaSuccess || cudaEventCreate(&ev1) != cudaSuccess)
             return TSE_ERR_LAUNCH;
     }

@@ -340,6 +340,39 @@ __global__ void eos_linear_kernel(EosLinear E, const double* T, double* rho, lon
     rho[t] = r;
 }
 
+// Declared per-cell property forms (constant, fourth-order polynomial in T),
+// optionally guarded: cells whose guard species equals guard_value keep their
+// value, as `if C[s] != v:` in a config callback does.
+struct EosForm {
+    int kind;
+    const double* guard;
+    double guard_value;
+    double c[5];
+};
+
+__global__ void eos_form_kernel(EosForm E, const double* T, double* out, long long n) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    if (E.guard && !(E.guard[t] != E.guard_value)) return;
+    double r;
+    if (E.kind == TSE_EOS_CONSTANT) {
+        r = E.c[0];
+    } else {
+        // c[4] + c[3]*T + c[2]*T**2 + c[1]*T**3 + c[0]*T**4, left to right,
+        // powers by repeated squaring: T**3 = T*(T*T), T**4 = (T*T)*(T*T) --
+        // the products numba emits for a literal integer exponent
+        const double x = T[t];
+        const double x2 = x * x;
+        const double x3 = x * x2;
+        const double x4 = x2 * x2;
+        r = E.c[4] + E.c[3] * x;
+        r = r + E.c[2] * x2;
+        r = r + E.c[1] * x3;
+        r = r + E.c[0] * x4;
+    }
+    out[t] = r;
+}
+
 inline unsigned grid_for(long long n) {
     long long b = (n + kBlock - 1) / kBlock;
     return (unsigned)(b < 1 ? 1 : b);
@@ -547,5 +580,21 @@ extern "C" int32_t tse_eos_linear(const TseGrid* grid, const double* const* h_C,
     E.tcoef = tcoef;
     E.T0 = T0;
     eos_linear_kernel<<<grid_for(n), kBlock, 0, (cudaStream_t)stream>>>(E, T, rho_f, n);
+    return cudaGetLastError() == cudaSuccess ? TSE_OK : TSE_ERR_LAUNCH;
+}
+
+extern "C" int32_t tse_eos_form(const TseGrid* grid, const TseEosForm* form, const double* T,
+                                const double* guard, double* out, void* stream) {
+    if (!grid || !form || !out) return TSE_ERR_ARG;
+    if (form->kind != TSE_EOS_CONSTANT && form->kind != TSE_EOS_POLY4_T) return TSE_ERR_ARG;
+    if (form->kind == TSE_EOS_POLY4_T && !T) return TSE_ERR_ARG;
+    const long long n = (long long)grid->nx * grid->ny * grid->nz;
+    if (n <= 0) return TSE_ERR_ARG;
+    EosForm E;
+    E.kind = form->kind;
+    E.guard = guard;
+    E.guard_value = form->guard_value;
+    for (int q = 0; q < 5; ++q) E.c[q] = form->coef[q];
+    eos_form_kernel<<<grid_for(n), kBlock, 0, (cudaStream_t)stream>>>(E, T, out, n);
     return cudaGetLastError() == cudaSuccess ? TSE_OK : TSE_ERR_LAUNCH;
 }

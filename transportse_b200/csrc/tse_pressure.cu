@@ -196,6 +196,7 @@ extern "C" int32_t tse_compute_P(const TseGrid* grid, const TsePressureArgs* arg
     SolveCtl ctl;
     ctl.L = L;
     ctl.Ncal = Ncal;
+    ctl.plain_sweep = args->sweep == 1;
     ctl.dt = args->dt_P;
     ctl.inc_it = args->inc_it;
     ctl.max_dt = args->max_dt;

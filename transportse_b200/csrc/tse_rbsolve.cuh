@@ -26,6 +26,7 @@ struct SolveCtl {
     int max_it;
     int pressure_schedule;      // 1: L2 every it below 50, then every 10th
     int stop_on_first;          // 1: converged after one it (omega == 0)
+    int plain_sweep;            // 1: plain-load kernel even where the staged one fits
     double* X[2];               // solution per colour
     const uint8_t* mask[2];
     double* partials;           // 2 doubles per block

@@ -368,15 +368,12 @@ __global__ void __launch_bounds__(kXThreads, TSE_X_MINB) rb_solve_tma_kernel(For
     }
 }
 
-// 1: the staged kernel wherever its stages fit (default); 0: plain loads
-int exact_sweep_mode();
-
 // Launch the staged loop when selected and its stages fit, TSE_X_MINB blocks
 // per SM (fewer for small grids: at least four chunks a block per half-sweep).
 // Returns TSE_OK, TSE_ERR_LAUNCH, or 1 when the plain kernel should run.
 template <class Form>
 inline int launch_rb_solve_tma(const Form& F, SolveCtl& ctl, cudaStream_t stream) {
-    if (exact_sweep_mode() != 1) return 1;
+    if (ctl.plain_sweep) return 1;
     int dev = 0, sms = 0, optin = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||

@@ -429,6 +429,7 @@ static int run_transport(const TseGrid* grid, const Args* a, double* X, TseSolve
     SolveCtl ctl;
     ctl.L = L;
     ctl.Ncal = w.Ncal;
+    ctl.plain_sweep = a->sweep == 1;
     ctl.dt = a->dt;
     ctl.inc_it = a->inc_it;
     ctl.max_dt = a->max_dt;

@@ -74,6 +74,9 @@ class Model:
         self.T_IMBLFLO = False
         self.last_status = None
         self.launches = 0
+        # FP64 solves' sweep kernel (args.sweep): 0 the bulk-copy staged
+        # kernel where its stages fit, 1 plain loads; same cell values
+        self.sweep = 0
         # optional per-solve timing: list of (kind, start event, end event,
         # status) appended by the solver entry points when enabled
         self.timing = False
@@ -217,6 +220,7 @@ class Model:
         a.dt_P, a.SOR, a.inc_it, a.max_dt, a.min_dt, a.P_conv = (
             float(dt_P), float(SOR), float(inc_it), float(max_dt), float(min_dt), float(P_conv))
         a.max_it = int(max_it)
+        a.sweep = int(self.sweep)
         ev = self._ev_start()
         self._solve("compute_P", a, a.P_conv)
         self.launches += 3
@@ -265,6 +269,7 @@ class Model:
             float(C_conv))
         a.max_it = int(max_it)
         a.imblflo = int(self.C_IMBLFLO)
+        a.sweep = int(self.sweep)
         ev = self._ev_start()
         self._solve("compute_C", a, a.conv)
         self.launches += 3
@@ -292,6 +297,7 @@ class Model:
             float(T_conv))
         a.max_it = int(max_it)
         a.imblflo = int(self.T_IMBLFLO)
+        a.sweep = int(self.sweep)
         ev = self._ev_start()
         self._solve("compute_T", a, a.conv)
         self.launches += 3
@@ -430,3 +436,32 @@ class Model:
         N.check(rc, "tse_eos_linear")
         self.launches += 1
         return rho_f
+
+    def eos_form(self, kind, coef, T, out, guard=None, guard_value=0.0):
+        """Declared constant or fourth-order-in-T property (tse_eos_form):
+        kind 'constant' (coef = value) or 'poly4_T' (coef = 5 coefficients,
+        highest power first as numpy.polyfit returns them); cells where
+        ``guard`` equals ``guard_value`` keep their value."""
+        f = N.TseEosForm()
+        if kind == "constant":
+            f.kind = N.TSE_EOS_CONSTANT
+            f.coef[0] = float(coef)
+        elif kind == "poly4_T":
+            c = [float(v) for v in coef]
+            if len(c) != 5:
+                raise ValueError("poly4_T takes 5 coefficients (numpy.polyfit order)")
+            f.kind = N.TSE_EOS_POLY4_T
+            for q in range(5):
+                f.coef[q] = c[q]
+        else:
+            raise ValueError("unknown EOS form %r" % (kind,))
+        f.guard_value = float(guard_value)
+        Tt = self._t(T) if T is not None else None
+        gt = self._t(guard) if guard is not None else None
+        rc = N.lib().tse_eos_form(ct.byref(self.grid), ct.byref(f),
+                                  self._p(Tt) if Tt is not None else None,
+                                  self._p(gt) if gt is not None else None,
+                                  self._p(out), self._stream())
+        N.check(rc, "tse_eos_form")
+        self.launches += 1
+        return out

@@ -253,6 +253,50 @@ def slice_2d_chem(nx=60, ny=1, nz=30, steps=40, per_cell=False):
     return m
 
 
+DYNBC_T1 = 40 * 86400.0    # s: the brine patch moves and a well starts
+DYNBC_T2 = 120 * 86400.0   # s: the well stops
+
+
+def dynbc_patch_and_well(t, bc_inc, P, T, C, BP, BT, BC, WP, WT, WC, Kx, Ky, Kz, rho_f, nue,
+                         c_f, cp_f, qx, phi, l_f, l_r):
+    """dynamic_bc of slice_2d_dynbc (the hook of tse.py:1448-1458), a pure
+    function of the time and bc_inc that changes its arrays in place:
+
+    * from DYNBC_T1 (bc_inc 0 -> 1): the Dirichlet brine patch on the top row
+      moves one third of the slice to the right (the old cells become free,
+      the new ones hold c = 1), and a well injects fluid low in the left part;
+    * from DYNBC_T2 (bc_inc 1 -> 2): the well stops and the left half of the
+      top row turns pressure-free (BP = 0).
+
+    Each change of bc_inc makes the driver re-run the equation of state."""
+    nx, ny, nz = P.shape
+    if bc_inc == 0 and t >= DYNBC_T1:
+        a, b = nx // 3, 2 * nx // 3
+        BC[a:b, :, nz - 1] = 0.0
+        BC[b:, :, nz - 1] = 1.0
+        C[b:, :, nz - 1, 0] = 1.0
+        WP[nx // 6, :, nz // 4] = 2.0e-7
+        bc_inc = 1
+    elif bc_inc == 1 and t >= DYNBC_T2:
+        WP[nx // 6, :, nz // 4] = 0.0
+        BP[: nx // 2, :, nz - 1] = 0.0
+        bc_inc = 2
+    return bc_inc, P, T, C, BP, BT, BC, WP, WT, WC, Kx, Ky, Kz
+
+
+def slice_2d_dynbc(nx=30, ny=1, nz=15, steps=60):
+    """slice_2d at 30 x 1 x 15 nodes with dynamic boundary conditions on
+    (DYNAMICBC, dynbc_patch_and_well): the brine patch moves and a well starts
+    after 40 days, the well stops and part of the top turns pressure-free
+    after 120 days; the linear EOS is re-run at each change."""
+    m = slice_2d(nx, ny, nz, steps)
+    m.__name__ = "slice_2d_dynbc"
+    m.DYNAMICBC = True
+    m.dynamic_bc = dynbc_patch_and_well
+    m.dt_max = 86400.0 * 10
+    return m
+
+
 def reservoir_3d(nx=256, ny=256, nz=128, seed=2024, steps=100):
     """Bottom-heated 3-D reservoir with a dense brine patch on top.
 
