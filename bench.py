@@ -65,6 +65,8 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the library's default sweep variant (chunk 512, 2 pipelines)")
     ap.add_argument("--kernel-only", choices=("fp64", "fp32dc"), default=None,
                     help="time one pressure solve of exactly --iters red+black iterations "
                          "(for isolated kernel timing and profiler captures)")
@@ -91,6 +93,9 @@ def parse_args():
     ap.add_argument("--batch-loop", choices=("device", "host"), default="device",
                     help="ensemble/serving, batched: the fused form's loop (device: one CUDA "
                          "graph per batch solve; host: a host round trip per sweep launch)")
+    ap.add_argument("--batch-cells", type=int, default=None,
+                    help="ensemble/serving, batched: largest sub-batch in cells (default: a "
+                         "third of L2 in FP32 corrections; 0: one batch)")
     ap.add_argument("--ensemble-models", type=int, default=512,
                     help="default run: models of the batched-ensemble key (0: leave it out)")
     ap.add_argument("--ensemble-steps", type=int, default=10,
@@ -109,6 +114,8 @@ def with_loop(runner, a):
     TseDcOptions.host_loop)."""
     if getattr(runner, "gate", None) is not None:
         runner.gate.host_loop = a.batch_loop == "host"
+        if a.batch_cells is not None:
+            runner.gate.batch_cells = int(a.batch_cells)
     return runner
 
 
@@ -355,6 +362,19 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------- CPU arm
+def cpu_model():
+    """The host CPU's model name (first /proc/cpuinfo entry)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
 def cpu_pressure_rate(shape, seconds):
     """The oracle's compute_P (C port of tse.py:647-742, OpenMP over all host
     threads) on the benchmark grid: single-iteration calls (P_conv = 1e300),
@@ -380,7 +400,7 @@ def cpu_pressure_rate(shape, seconds):
         if el >= seconds and calls >= 2:
             break
     return {"value": active * calls / el, "unit": "cell-updates/s", "cores": cores,
-            "kind": "port",
+            "kind": "port", "cpu_model": cpu_model(),
             "sample": "%d single-iteration compute_P calls (red+black sweep, copy, L2) on the "
                       "%dx%dx%d grid, %.1f s" % ((calls,) + tuple(shape) + (el,))}
 
@@ -402,7 +422,8 @@ def run_reference_arm(a, rank):
         "dtype": "f64", "data": "synthetic",
         "config": {"workload": "reservoir_3d %dx%dx%d pressure SOR sweeps" % shape},
         "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": info["cores"],
-                         "kind": info["kind"], "sample": info["sample"]},
+                         "kind": info["kind"], "cpu_model": info["cpu_model"],
+                         "sample": info["sample"]},
         "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0}}))
 
@@ -520,7 +541,7 @@ def roofline(res, precision, peak, peak_kind):
         if not res["n_s"]:
             return None
         units, ms, n = res["s_units"], res["s_ms"], res["n_s"]
-        name = "dc_sweep_tma_kernel<4, 2> (FP32 correction sweeps, bulk-copy pipelines)"
+        name = "dc_sweep_tma_kernel<ring, pipes, chunk> (FP32 correction sweeps, bulk-copy pipelines; variant in autotune)"
     else:
         if not res["n_p"]:
             return None
@@ -629,6 +650,12 @@ def main():
     sim = Simulation(workloads.reservoir_3d(*shape), device=dev, precision="fp32dc")
     if a.dc_cycle:
         sim.M.dc_cycle = int(a.dc_cycle)
+    tune = None
+    if not a.no_autotune:
+        # the staged sweep's chunk / ring / pipelines for this grid, timed on
+        # its own pressure solve (results do not depend on the choice)
+        from transportse_b200 import autotune
+        tune = autotune.tune_sweep(sim)
     for _ in range(a.warmup):
         sim.run(max_steps=1)
     res = timed_steps(ctx, sim, a.steps, ClockSampler(local))
@@ -687,6 +714,7 @@ def main():
                        "parallelism": "replicas" if world > 1 else "single",
                        "l2": "working set > L2 (no flush)"},
             "gpu_launches": int(res["launches"]), "clocks": res["clocks"], "e2e": e2e,
+            "autotune": tune,
             # pressure SOR / species / heat separately: each solve call's event
             # time (sweeps, residuals, set-up) and its cell-updates
             "rates_by_solve": res["rates_by_solve"],

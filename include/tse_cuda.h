@@ -167,6 +167,23 @@ typedef struct TseDcOptions {
                                  events, x += d, residuals); in the device-driven
                                  loop sweep_ms is then the sweep kernel's own
                                  time, taken with the device's global timer */
+    int32_t chunk;            /* in/out, single-model forms: the staged sweep's
+                                 chunk of cells (256, 512, 1024; else 512) --
+                                 on return the variant that ran, 0 for the
+                                 plain-load sweep (no stages fit) */
+    int32_t ring;             /* in/out: stages a pipeline (2..4; else as many
+                                 as fit, up to 4) */
+    int32_t pipes;            /* in/out: pipelines a block (1: two blocks per
+                                 SM; else 2: one block per SM) */
+    int32_t reserved2;
+    int64_t active_cells;     /* in, batched fused form with the device-driven
+                                 loop: cells (both colours, padding included)
+                                 solving at once; the items wait in index order
+                                 and join as earlier ones finish (the first
+                                 waiting item always when none runs); <= 0:
+                                 every item from the start.  Each model's
+                                 results are those of its solve alone either
+                                 way. */
 } TseDcOptions;
 int32_t tse_compute_P_dc(const TseGrid *grid, const TsePressureArgs *args,
                          TseDcOptions *opts, TseSolveStatus *d_status,

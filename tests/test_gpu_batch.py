@@ -16,11 +16,11 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-6
 
 
-def _run_members(fns, device, cluster=0, host_loop=False):
+def _run_members(fns, device, cluster=0, host_loop=False, batch_cells=None):
     """Run fns[i](gate) on threads of their own, each on its own stream, all
     joined to one gate before any starts (so the first solves batch)."""
     from transportse_b200.batch import BatchGate
-    gate = BatchGate(device, cluster=cluster, host_loop=host_loop)
+    gate = BatchGate(device, cluster=cluster, host_loop=host_loop, batch_cells=batch_cells)
     out = [None] * len(fns)
     errs = []
     for _ in fns:
@@ -140,6 +140,41 @@ def test_device_loop_equals_host_loop(kw, cuda_device):
         used[mode] = (g1.value - g0.value, h1.value - h0.value)
     assert used[1] == (1, 0) and used[0] == (0, 1), used
     for i, (a, b) in enumerate(zip(out[1], out[0])):
+        assert (a[0], a[1], a[4], a[5]) == (b[0], b[1], b[4], b[5]), SHAPES[i]
+        assert numpy.array_equal(a[2], b[2]), SHAPES[i]
+
+
+@pytest.mark.parametrize("kw", [
+    dict(SOR=1.7, max_it=20000, inc_it=1.25, max_dt=1e5, min_dt=1e-8, P_conv=1e-10),
+    dict(SOR=1.7, max_it=25, inc_it=1.25, max_dt=1e5, min_dt=400.0, P_conv=1e-12)])
+def test_device_loop_admitting_models_equals_host_loop(kw, cuda_device):
+    """A cell budget below the batch's total (TseDcOptions.active_cells): the
+    device-driven loop starts with the largest models and admits the others
+    into the running loop as earlier ones finish; each admitted model counts
+    its own iterations and checks from its admission.  Every model's
+    pressure, t, dt, convergence flag and iteration count equal the host
+    loop's (all models at once, no budget) bit for bit -- through cycle ends,
+    refreshes and dt halvings -- and the batch still goes out as one call."""
+    cases_ = [_pressure_case(s, 7 + i) for i, s in enumerate(SHAPES)]
+
+    def member(i):
+        cfg, P, rest = cases_[i]
+
+        def fn(gate):
+            m = model_for(cfg, cuda_device, "fp32dc")
+            m.batch_gate = gate
+            return NumpyKernels(m).compute_P(P.copy(), *rest, **kw)
+        return fn
+
+    ref, _ = _run_members([member(i) for i in range(len(SHAPES))], cuda_device, host_loop=True,
+                          batch_cells=0)
+    # 5,000 cells: the 28,800- and 11,781-cell models run alone, the rest in
+    # waves behind them
+    got, gate = _run_members([member(i) for i in range(len(SHAPES))], cuda_device,
+                             batch_cells=5000)
+    st = gate.stats()
+    assert st["launches"]["compute_P"] == 1 and st["solves"]["compute_P"] == len(SHAPES)
+    for i, (a, b) in enumerate(zip(got, ref)):
         assert (a[0], a[1], a[4], a[5]) == (b[0], b[1], b[4], b[5]), SHAPES[i]
         assert numpy.array_equal(a[2], b[2]), SHAPES[i]
 

@@ -423,7 +423,10 @@ def test_staged_sweep_copies_stay_aligned_and_in_bounds():
     Hmax = max((nz + (nz & 1)) // 2 for _, _, nz in shapes)
     for nx, ny, nz in shapes:
         H = (nz + (nz & 1)) // 2
-        assert _staged_copies_ok(nx, ny, nz, H), (nx, ny, nz)
+        # every compiled chunk size of the single-model sweep (the autotuner's
+        # choices); the fused batch keeps 512
+        for C in (256, 512, 1024):
+            assert _staged_copies_ok(nx, ny, nz, H, C), (nx, ny, nz, C)
         assert _staged_copies_ok(nx, ny, nz, Hmax), (nx, ny, nz, "fused")
 
 
@@ -535,3 +538,29 @@ def test_server_cancels_pending_requests():
     assert a.cancelled and a.done.is_set() and a.error is not None
     assert s.cancel(0) is False and s.cancel(7) is False
     assert [item[1] for item in s.pending] == [1] and not b.done.is_set()
+
+
+def test_batch_gate_sub_batches_by_cell_budget():
+    """The fused form's sub-batches: every request once, sorted by size, each
+    sub-batch within the budget unless a single model alone exceeds it; no
+    split under the budget, with a cluster form or with the budget off."""
+    import types
+    from transportse_b200 import batch as B
+    gate = B.BatchGate("cpu", batch_cells=1000)
+    rng = numpy.random.default_rng(4)
+    reqs = []
+    for i in range(40):
+        n = int(rng.integers(2, 12))
+        reqs.append(types.SimpleNamespace(grid=types.SimpleNamespace(nx=n, ny=n, nz=3), i=i))
+    cells = lambda r: r.grid.nx * r.grid.ny * r.grid.nz
+    subs = gate._subbatches(reqs)
+    flat = [r for s in subs for r in s]
+    assert sorted(r.i for r in flat) == list(range(40))
+    assert [cells(r) for r in flat] == sorted(cells(r) for r in reqs)
+    for s in subs:
+        assert sum(cells(r) for r in s) <= 1000 or len(s) == 1
+    assert len(subs) > 1
+    assert gate._subbatches(reqs[:3]) == [reqs[:3]]
+    assert B.BatchGate("cpu", batch_cells=0)._subbatches(reqs) == [reqs]
+    assert B.BatchGate("cpu", cluster=8, batch_cells=1000)._subbatches(reqs) == [reqs]
+    assert B.default_batch_cells("cpu") == 0

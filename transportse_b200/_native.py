@@ -79,7 +79,8 @@ class TseDcOptions(ct.Structure):
     _fields_ = [("cycle", ct.c_int32), ("max_blocks", ct.c_int32), ("timing", ct.c_int32),
                 ("sweep_launches", ct.c_int32), ("sweep_iterations", ct.c_int64),
                 ("sweep_ms", ct.c_double), ("host_loop", ct.c_int32), ("reserved", ct.c_int32),
-                ("loop_ms", ct.c_double)]
+                ("loop_ms", ct.c_double), ("chunk", ct.c_int32), ("ring", ct.c_int32),
+                ("pipes", ct.c_int32), ("reserved2", ct.c_int32), ("active_cells", ct.c_int64)]
 
 
 def _batch_item(args_type):

@@ -248,10 +248,9 @@ __device__ void cluster_dc_solve(cg::cluster_group& cl, const BatchItem<Form>& i
     const Layout& L = c.L;
     const long long nat = (long long)L.nx * L.ny * L.nz;
     for (long long q = g; q < nat; q += step) {
-        const int k = (int)(q % L.nz);
-        const long long row = q / L.nz;
-        const int j = (int)(row % L.ny);
-        const int i = (int)(row / L.ny);
+        int i, j, k;
+        long long row;
+        grid_coords(q, L.ny, L.nz, i, j, k, row);
         const long long m = (row * L.nzp + k) >> 1;
         it.X_out[q] = ((i + j + k) & 1) ? __ldcg(c.X[1] + m) : __ldcg(c.X[0] + m);
     }
@@ -367,7 +366,8 @@ struct FusedItem {
     DcCtl c;
     long long cfirst, nchunks;   // this model's chunks in the table
     int inner;                   // iterations since its last residual, at launch
-    int pad;
+    int age0;                    // its own iteration count at launch (models
+                                 // admitted later count from their admission)
 };
 
 struct FusedChunk {
@@ -387,7 +387,18 @@ struct FusedArgs {
     int g_max;           // iterations this launch runs at most
     int num_it0;         // the models' iteration count at launch
     int pressure_schedule;
+    // the pressure check schedule (every iteration below 50, then every 10th)
+    // of the youngest model and of every model's phase: at launch iteration
+    // g some model checks if young + g < 50 or bit g % 10 of mask10 is set
+    int young;
+    int mask10;
 };
+
+// the check schedule of a model of age a (its own iterations) under the
+// pressure schedule (tse.py:719-723) or the transport one (every iteration)
+__device__ __forceinline__ bool model_checks(int pressure_schedule, int a) {
+    return pressure_schedule ? (a < 50 || a % 10 == 0) : true;
+}
 
 // one model's decision after global iteration g (thread 0 of its block)
 __device__ void fused_decide(const FusedItem& I, int g, int num_it, bool check, double s1, double s3,
@@ -477,8 +488,9 @@ __device__ __forceinline__ void fused_sweep_body(const FusedArgs& A, const TmaSt
     unsigned bars = 0;   // device-wide barriers passed (A.bar->count, zeroed per launch)
     bool ok = true;
     for (int g = 1; g <= A.g_max && ok; ++g) {
-        const int num_it = A.num_it0 + g;
-        const bool check = A.pressure_schedule ? (num_it < 50 || num_it % 10 == 0) : true;
+        // whether any model checks at this iteration (the chunks then store
+        // their sums; each model's decision uses its own schedule)
+        const bool check = !A.pressure_schedule || A.young + g < 50 || ((A.mask10 >> (g % 10)) & 1);
         const bool last = g == A.g_max;
         for (int col = 0; col < 2 && ok; ++col) {
             if (producer) {
@@ -577,8 +589,10 @@ __device__ __forceinline__ void fused_sweep_body(const FusedArgs& A, const TmaSt
         if (check || last) {
             for (int it = (int)b; it < A.nitems; it += (int)nb) {
                 const FusedItem& I = A.items[it];
+                const int age = I.age0 + g;
+                const bool mcheck = check && model_checks(A.pressure_schedule, age);
                 double s1 = 0.0, s3 = 0.0;
-                if (check)
+                if (mcheck)
                     for (long long k = tid; k < I.nchunks; k += blockDim.x) {
                         const double2* pk = A.cpart + 8 * (I.cfirst + k);   // 2 colours x 4 warps
 #pragma unroll
@@ -590,7 +604,7 @@ __device__ __forceinline__ void fused_sweep_body(const FusedArgs& A, const TmaSt
                     }
                 s1 = block_sum<kFusedThreads>(s1, sh);
                 s3 = block_sum<kFusedThreads>(s3, sh);
-                if (tid == 0) fused_decide(I, g, num_it, check, s1, s3, A.any_event);
+                if (tid == 0) fused_decide(I, g, age, mcheck, s1, s3, A.any_event);
                 __syncthreads();
             }
             ok = count_sync(&A.bar->count, ++bars * nb, A.bar);
@@ -764,6 +778,7 @@ static int run_fused(std::vector<BatchItem<Form>>& v, TseDcOptions* opts, void* 
             const long long nc = (v[i].c.L.Nc + kTmaChunk - 1) / kTmaChunk;
             I.nchunks = nc;
             I.inner = inner[i];
+            I.age0 = st[i].num_it;
             for (long long q = 0; q < nc; ++q) hchunks.push_back(FusedChunk{q * kTmaChunk, k, 0});
             hitems.push_back(I);
         }
@@ -780,6 +795,9 @@ static int run_fused(std::vector<BatchItem<Form>>& v, TseDcOptions* opts, void* 
         A.g_max = g_max;
         A.num_it0 = num_it;
         A.pressure_schedule = v[0].c.pressure_schedule;
+        // every model of the host loop starts together: one age, one phase
+        A.young = num_it;
+        A.mask10 = 1 << ((10 - num_it % 10) % 10);
         long long nb = (long long)sms * per_sm;
         if (nb > nch) nb = nch;
         if (nb > kMaxBlocks) nb = kMaxBlocks;
@@ -888,7 +906,7 @@ static int run_fused(std::vector<BatchItem<Form>>& v, TseDcOptions* opts, void* 
 
 struct FusedCtl {
     int n;                   // models of the batch
-    int nactive;             // models still solving, after the last events pass
+    int nactive;             // models solving or waiting, after the last events pass
     int num_it;              // the models' global iteration count
     int failed;              // a sweep reported EV_ERROR
     int runs;                // loop-body runs in the current graph launch
@@ -896,6 +914,7 @@ struct FusedCtl {
     long long iterations;    // global iterations over the whole solve
     long long resid_total;   // residual blocks of the current body run, all models
     unsigned long long sweep_ns;   // summed duration of the sweep launches
+    long long budget;        // cells (both colours) active at once; 0: every model
 };
 
 __device__ void fused_add_sweep_ns(FusedCtl* ctl, unsigned long long ns) { ctl->sweep_ns += ns; }
@@ -906,6 +925,8 @@ struct FusedModel {
     long long nchunks;       // ceil(Nc / kTmaChunk)
     int active;              // 1 while solving
     int inner;               // iterations since the model's last residual
+    int waiting;             // 1 until admitted (a cell budget holds it back)
+    int pad;
 };
 
 enum : int { ACT_APPLY = 1, ACT_HALVE = 2, ACT_RESID = 4 };
@@ -939,23 +960,64 @@ __device__ V block_inclusive_scan(V v, V* sh, V* total) {
     return v;
 }
 
-// the active models in index order, their iteration limit for the launch
-// (run_fused's g_max), their chunk ranges and the sweep's arguments
-__global__ void __launch_bounds__(kPlanThreads) fused_plan_kernel(const FusedCtl* ctl, const FusedModel* models,
+// Admission, then the active models in index order, their iteration limit
+// for the launch (run_fused's g_max), their chunk ranges and the sweep's
+// arguments.  Admission (a cell budget): waiting models join in index order
+// while the active cells stay within ctl->budget -- the first waiting model
+// always, when none is active -- so models that converge early hand their
+// share of the GPU to the next ones instead of leaving it idle until the
+// slowest model of the batch is done.  An admitted model counts its own
+// iterations from 0 (its state record is its solve's from the start), so
+// its iterations, checks and decisions are those of its solve alone.
+__global__ void __launch_bounds__(kPlanThreads) fused_plan_kernel(const FusedCtl* ctl, FusedModel* models,
                                                                   FusedItem* items, int* idx, FusedArgs* args,
                                                                   FusedChunk* chunks, double2* cpart,
                                                                   int* any_event, GridBarrier* bar) {
     __shared__ long long sh_ll[32];
     __shared__ int sh_i[32];
-    __shared__ int s_gmax, s_base_k;
-    __shared__ long long s_base_ch;
+    __shared__ int s_gmax, s_base_k, s_young, s_mask;
+    __shared__ long long s_base_ch, s_active_cells, s_base_w;
     const int n = ctl->n;
     if (threadIdx.x == 0) {
         s_gmax = 1 << 30;
         s_base_k = 0;
         s_base_ch = 0;
+        s_active_cells = 0;
+        s_base_w = 0;
+        s_young = 1 << 30;
+        s_mask = 0;
     }
     __syncthreads();
+    if (ctl->budget > 0) {
+        // cells of the active models
+        for (int base = 0; base < n; base += kPlanThreads) {
+            const int i = base + threadIdx.x;
+            const long long cells = (i < n && models[i].active) ? 2 * models[i].c.L.Nc : 0;
+            long long tot;
+            block_inclusive_scan<long long>(cells, sh_ll, &tot);
+            if (threadIdx.x == 0) s_active_cells += tot;
+            __syncthreads();
+        }
+        // waiting models in index order, while they fit
+        const long long room = ctl->budget - s_active_cells;
+        const bool none = s_active_cells == 0;
+        for (int base = 0; base < n; base += kPlanThreads) {
+            const int i = base + threadIdx.x;
+            const bool w = i < n && models[i].waiting;
+            const long long cells = w ? 2 * models[i].c.L.Nc : 0;
+            long long tot;
+            const long long p = block_inclusive_scan<long long>(cells, sh_ll, &tot);
+            const long long incl = s_base_w + p;
+            if (w && (incl <= room || (none && incl == cells))) {
+                models[i].waiting = 0;
+                models[i].active = 1;
+                models[i].inner = 0;
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) s_base_w += tot;
+            __syncthreads();
+        }
+    }
     for (int base = 0; base < n; base += kPlanThreads) {
         const int i = base + threadIdx.x;
         int a = 0;
@@ -970,6 +1032,8 @@ __global__ void __launch_bounds__(kPlanThreads) fused_plan_kernel(const FusedCtl
             lim = h < lim ? h : lim;
             if (st->dt <= M.c.min_dt) lim = 1;
             atomicMin(&s_gmax, lim);
+            atomicMin(&s_young, st->num_it);
+            atomicOr(&s_mask, 1 << ((10 - st->num_it % 10) % 10));
         }
         int tot_a;
         long long tot_c;
@@ -982,7 +1046,7 @@ __global__ void __launch_bounds__(kPlanThreads) fused_plan_kernel(const FusedCtl
             I.cfirst = s_base_ch + pc - nc;
             I.nchunks = nc;
             I.inner = models[i].inner;
-            I.pad = 0;
+            I.age0 = models[i].c.st->num_it;
             items[k] = I;
             idx[k] = i;
         }
@@ -1005,6 +1069,8 @@ __global__ void __launch_bounds__(kPlanThreads) fused_plan_kernel(const FusedCtl
         A.g_max = s_gmax < 1 ? 1 : s_gmax;
         A.num_it0 = ctl->num_it;
         A.pressure_schedule = s_base_k > 0 ? items[0].c.pressure_schedule : 0;
+        A.young = s_young;
+        A.mask10 = s_mask;
         *args = A;
         *any_event = 0;
         bar->count = 0;
@@ -1046,7 +1112,9 @@ __global__ void __launch_bounds__(kPlanThreads) fused_events_kernel(FusedCtl* ct
     const FusedArgs A = *args;
     const int na = A.nitems;
     if (threadIdx.x == 0) {
-        s_ran = na > 0 ? A.items[0].c.st->num_it - ctl->num_it : 0;
+        // every model decides at the launch's last iteration: its own count
+        // then tells how many iterations the launch ran
+        s_ran = na > 0 ? A.items[0].c.st->num_it - A.items[0].age0 : 0;
         s_failed = 0;
         s_active = 0;
         s_base = 0;
@@ -1084,8 +1152,12 @@ __global__ void __launch_bounds__(kPlanThreads) fused_events_kernel(FusedCtl* ct
     // a failure ends every model, after this pass's steps (as run_fused)
     const bool failed = s_failed != 0;
     for (int i = threadIdx.x; i < ctl->n; i += blockDim.x) {
-        if (failed) models[i].active = 0;
-        else if (models[i].active) atomicAdd(&s_active, 1);
+        if (failed) {
+            models[i].active = 0;
+            models[i].waiting = 0;
+        } else if (models[i].active || models[i].waiting) {
+            atomicAdd(&s_active, 1);
+        }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -1186,6 +1258,9 @@ static int run_fused_graph(std::vector<BatchItem<Form>>& v, TseDcOptions* opts, 
                            cudaStream_t stream) {
     if ((opts && opts->host_loop == 1) || stream == nullptr) return 1;
     const int n = (int)v.size();
+    // cells (both colours) active at once; below the batch's total, waiting
+    // models are admitted as others finish
+    long long budget = (opts && opts->active_cells > 0) ? opts->active_cells : 0;
     long long cells = 0;
     int Hmax = 0;
     for (auto& it : v) {
@@ -1313,7 +1388,9 @@ static int run_fused_graph(std::vector<BatchItem<Form>>& v, TseDcOptions* opts, 
         memset(&hm[i], 0, sizeof(FusedModel));
         hm[i].c = v[i].c;
         hm[i].nchunks = (v[i].c.L.Nc + kTmaChunk - 1) / kTmaChunk;
-        hm[i].active = 1;
+        // with a cell budget every model waits for the first plan to admit it
+        hm[i].active = budget > 0 ? 0 : 1;
+        hm[i].waiting = budget > 0 ? 1 : 0;
         hm[i].inner = 0;
         hf[i] = v[i].F;
     }
@@ -1321,6 +1398,7 @@ static int run_fused_graph(std::vector<BatchItem<Form>>& v, TseDcOptions* opts, 
     memset(&hc, 0, sizeof(hc));
     hc.n = n;
     hc.nactive = n;
+    hc.budget = budget;
     // pageable sources: staged before the calls return
     if (rc == TSE_OK &&
         (cudaMemcpyAsync(d_models, hm.data(), sizeof(FusedModel) * n, cudaMemcpyHostToDevice, stream) !=

@@ -38,6 +38,27 @@ __device__ __forceinline__ double nmin(double a, double b) {
     return (a != a) ? a : ((b != b) ? b : ((b < a) ? b : a));
 }
 
+// The grid coordinates of linear index t = (i*ny + j)*nz + k (nz may be a
+// padded column height): 32-bit divisions while t fits, which is every grid
+// below 2^32 cells -- a 64-bit division is several times the instructions.
+__device__ __forceinline__ void grid_coords(long long t, int ny, int nz, int& i, int& j, int& k,
+                                            long long& row) {
+    if (t <= 0xffffffffLL) {
+        const unsigned u = (unsigned)t, r = u / (unsigned)nz;
+        k = (int)(u - r * (unsigned)nz);
+        row = r;
+        const unsigned ii = r / (unsigned)ny;
+        j = (int)(r - ii * (unsigned)ny);
+        i = (int)ii;
+    } else {
+        row = t / nz;
+        k = (int)(t - row * nz);
+        const long long ii = row / ny;
+        j = (int)(row - ii * ny);
+        i = (int)ii;
+    }
+}
+
 __device__ __forceinline__ uint64_t globaltimer() {
     uint64_t t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));

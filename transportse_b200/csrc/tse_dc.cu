@@ -248,9 +248,11 @@ __global__ void __launch_bounds__(kSweepBlock, kSweepMinBlocks) dc_sweep_kernel(
 
 // ------------------------------------------------ FP32 sweeps, bulk-copy staged
 // (the staging pieces are in tse_dc.cuh)
-template <int RING, int PIPES>
+template <int RING, int PIPES, int CHUNK>
 __global__ void __launch_bounds__(DcLayout<PIPES>::kThreads, DcLayout<PIPES>::kMinBlocks)
     dc_sweep_tma_kernel(DcCtl c, TmaStage T) {
+    static_assert(CHUNK % kTmaGroup == 0 && CHUNK <= kDcMaxChunk, "whole cells per thread, in the margins");
+    constexpr int kCellsPerThread = CHUNK / kTmaGroup;
     constexpr int kPipes = PIPES;
     constexpr int kThreads = DcLayout<PIPES>::kThreads;
     extern __shared__ __align__(128) unsigned char smem[];
@@ -271,7 +273,7 @@ __global__ void __launch_bounds__(DcLayout<PIPES>::kThreads, DcLayout<PIPES>::kM
     constexpr int kGroupsPerPipe = DcLayout<PIPES>::kGroupsPerPipe;
     constexpr unsigned ring = RING;                     // stages of a ring (T.stages / PIPES)
     const unsigned ring0 = (unsigned)pipe * ring;    // the pipeline's first stage
-    const long long Nc = c.L.Nc, N = c.Ncal, SX = c.L.SX, C = kTmaChunk;
+    const long long Nc = c.L.Nc, N = c.Ncal, SX = c.L.SX, C = CHUNK;
     const int H = c.L.H;
     const long long nch = (Nc + C - 1) / C;
     const long long mine = nch > (long long)b ? (nch - 1 - b) / nb + 1 : 0;   // chunks of this block
@@ -396,7 +398,7 @@ __global__ void __launch_bounds__(DcLayout<PIPES>::kThreads, DcLayout<PIPES>::kM
                     const float* wxm = reinterpret_cast<const float*>(stg + T.wxm);
                     float* out = dw + m0;
 #pragma unroll
-                    for (int r = 0; r < kTmaCellsPerThread; ++r) {
+                    for (int r = 0; r < kCellsPerThread; ++r) {
                         const int l = gt + r * kTmaGroup;
                         if (l < nval) {
                             const float2 k01 = rec[3 * l], k23 = rec[3 * l + 1], k45 = rec[3 * l + 2];
@@ -574,14 +576,23 @@ static size_t tma_max_smem() {
 // blocks of the staged sweep: as many as fit (dynamic shared memory
 // included), at most one per chunk of a colour; 0 when the stages for this
 // grid's windows do not fit (the plain sweep kernel runs instead)
-// the instantiation for rings of `ring` stages (2 .. 4)
-static const void* tma_kernel(int ring) {
-    return ring <= 2 ? (const void*)dc_sweep_tma_kernel<2, kDcPipes>
-         : ring == 3 ? (const void*)dc_sweep_tma_kernel<3, kDcPipes>
-                     : (const void*)dc_sweep_tma_kernel<4, kDcPipes>;
+// the instantiation for rings of `ring` stages (2 .. 4), `pipes` pipelines
+// per block (1: two blocks per SM) and chunks of `chunk` cells
+template <int PIPES, int CHUNK>
+static const void* tma_kernel_r(int ring) {
+    return ring <= 2 ? (const void*)dc_sweep_tma_kernel<2, PIPES, CHUNK>
+         : ring == 3 ? (const void*)dc_sweep_tma_kernel<3, PIPES, CHUNK>
+                     : (const void*)dc_sweep_tma_kernel<4, PIPES, CHUNK>;
+}
+static const void* tma_kernel(int ring, int pipes, int chunk) {
+    if (pipes == 1)
+        return chunk == 256 ? tma_kernel_r<1, 256>(ring) : chunk == 1024 ? tma_kernel_r<1, 1024>(ring)
+                                                                         : tma_kernel_r<1, 512>(ring);
+    return chunk == 256 ? tma_kernel_r<2, 256>(ring) : chunk == 1024 ? tma_kernel_r<2, 1024>(ring)
+                                                                     : tma_kernel_r<2, 512>(ring);
 }
 
-static int tma_blocks(long long Nc, int cap, size_t smem, const void* kernel, int threads) {
+static int tma_blocks(long long Nc, int cap, size_t smem, const void* kernel, int threads, int chunk) {
     const size_t ceil_smem = tma_max_smem();
     if (!TSE_SWEEP_TMA || smem == 0 || smem > ceil_smem) return 0;
     int dev = 0, sms = 0, per_sm = 0;
@@ -598,7 +609,7 @@ static int tma_blocks(long long Nc, int cap, size_t smem, const void* kernel, in
         return 0;
     }
     long long nb = (long long)sms * per_sm;
-    const long long nch = (Nc + kTmaChunk - 1) / kTmaChunk;
+    const long long nch = (Nc + chunk - 1) / chunk;
     if (nb > nch) nb = nch;
     if (nb > kMaxBlocks / 2) nb = kMaxBlocks / 2;
     if (cap > 0 && nb > cap) nb = cap;
@@ -633,18 +644,30 @@ static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, 
     if (cudaGetLastError() != cudaSuccess) return TSE_ERR_LAUNCH;
     const long long cells2 = 2 * S.L.Nc;
     const unsigned gcells = (unsigned)((cells2 + kBlock - 1) / kBlock);
-    TmaStage T = tma_stage(S.L.H);
-    // as many stages as fit, up to 4 a ring, an equal ring per pipeline
-    const int pipes = kDcPipes;
+    // the staged sweep's variant: chunk size, pipelines per block and ring
+    // length from the call's options (0: 512 cells, 2 pipelines, as many
+    // stages as fit up to 4 a ring)
+    const int chunk = (opts && (opts->chunk == 256 || opts->chunk == 1024)) ? opts->chunk : 512;
+    const int pipes = (opts && opts->pipes == 1) ? 1 : kDcPipes;
+    const int want_ring = (opts && opts->ring >= 2 && opts->ring <= kDcMaxRing) ? opts->ring : kDcMaxRing;
+    TmaStage T = tma_stage(S.L.H, chunk);
     {
-        int st = (int)std::min<size_t>((size_t)(kDcMaxRing * pipes), tma_max_smem() / (size_t)T.bytes);
+        // one pipeline per block runs two blocks per SM: each gets half
+        const size_t room = tma_max_smem() / (pipes == 1 ? 2 : 1);
+        int st = (int)std::min<size_t>((size_t)(want_ring * pipes), room / (size_t)T.bytes);
         st -= st % pipes;
         T.stages = st >= 2 * pipes ? st : 0;
     }
     const size_t tma_smem = (size_t)T.stages * T.bytes;
     const int tma_threads = kTmaConsumers + 32 * pipes;
-    const void* tma_k = T.stages > 0 ? tma_kernel(T.stages / pipes) : nullptr;
-    const int nb_tma = tma_k ? tma_blocks(S.L.Nc, cap, tma_smem, tma_k, tma_threads) : 0;
+    const void* tma_k = T.stages > 0 ? tma_kernel(T.stages / pipes, pipes, chunk) : nullptr;
+    const int nb_tma = tma_k ? tma_blocks(S.L.Nc, cap, tma_smem, tma_k, tma_threads, chunk) : 0;
+    if (opts) {
+        // the variant that ran (0 when the plain-load sweep did)
+        opts->chunk = nb_tma > 0 ? chunk : 0;
+        opts->pipes = nb_tma > 0 ? pipes : 0;
+        opts->ring = nb_tma > 0 ? T.stages / pipes : 0;
+    }
     const int nb = nb_tma > 0 ? nb_tma : sweep_blocks(S.L.Nc, cap);
     dc_scale_kernel<<<gcells, kBlock, 0, stream>>>(S.F, c);
     if (cudaGetLastError() != cudaSuccess) return TSE_ERR_LAUNCH;

@@ -220,11 +220,12 @@ struct TmaStage {
     int rec, rp, msk, dw, wz, wxp, wxm, bytes;
     int lz, lx;   // window lengths in floats
     int stages;   // stages of the launch, over all its pipelines (set by the launcher)
+    int chunk;    // cells a chunk (256, 512 or 1024)
 };
 
-__host__ __device__ inline TmaStage tma_stage(int H) {
+__host__ __device__ inline TmaStage tma_stage(int H, int C = kTmaChunk) {
     TmaStage t;
-    const int C = kTmaChunk;
+    t.chunk = C;
     t.rec = 0;
     t.rp = 24 * C;
     t.msk = t.rp + 4 * C;
@@ -273,7 +274,7 @@ __device__ __forceinline__ void tma_issue_windows(const DcCtl& c, const TmaStage
     const long long xms = (m0 - SX) & ~3LL;
     // this model's own window length (a batch's stage slot is sized for its
     // largest H; a longer copy could leave this model's margins)
-    const unsigned b_z = (unsigned)(4 * tma_stage(H).lz), b_x = (unsigned)(4 * T.lx);
+    const unsigned b_z = (unsigned)(4 * tma_stage(H, T.chunk).lz), b_x = (unsigned)(4 * T.lx);
     const uint64_t last = l2_evict_last();
     mbar_expect_tx(bar, b_z + 2 * b_x);
     bulk_g2s_hint(stage + T.wz, dq + zs, b_z, bar, last);

@@ -8,10 +8,8 @@ namespace tse {
 constexpr int kRedBlocks = 1024;   // fixed partial count: deterministic reductions
 
 __device__ __forceinline__ void decode(long long t, int ny, int nz, int& i, int& j, int& k) {
-    k = (int)(t % nz);
-    const long long row = t / nz;
-    j = (int)(row % ny);
-    i = (int)(row / ny);
+    long long row;
+    grid_coords(t, ny, nz, i, j, k, row);
 }
 
 // compute_q (tse.py:744-780); q on the last plane of each axis is not written

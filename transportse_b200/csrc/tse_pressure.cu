@@ -32,10 +32,9 @@ __global__ void assemble_p_kernel(TseGrid g, TsePressureArgs a, PressureForm F, 
     const long long total = (long long)L.nx * L.ny * L.nzp;
     if (t >= total) return;
     const int nx = L.nx, ny = L.ny, nz = L.nz;
-    const int k = (int)(t % L.nzp);
-    const long long row = t / L.nzp;
-    const int j = (int)(row % ny);
-    const int i = (int)(row / ny);
+    int i, j, k;
+    long long row;
+    grid_coords(t, ny, L.nzp, i, j, k, row);
     const long long m = t >> 1;
     const int col = (i + j + k) & 1;
     double* b = F.arr[col];
@@ -112,10 +111,9 @@ __global__ void unpack_kernel(double* out, const double* X0, const double* X1, L
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long total = (long long)L.nx * L.ny * L.nz;
     if (t >= total) return;
-    const int k = (int)(t % L.nz);
-    const long long row = t / L.nz;
-    const int j = (int)(row % L.ny);
-    const int i = (int)(row / L.ny);
+    int i, j, k;
+    long long row;
+    grid_coords(t, L.ny, L.nz, i, j, k, row);
     const long long m = (row * L.nzp + k) >> 1;
     out[t] = ((i + j + k) & 1) ? X1[m] : X0[m];
 }

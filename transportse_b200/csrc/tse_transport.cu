@@ -99,10 +99,8 @@ struct CellIdx {
 __device__ __forceinline__ bool decode_padded(long long t, const Layout& L, CellIdx& x) {
     const long long total = (long long)L.nx * L.ny * L.nzp;
     if (t >= total) return false;
-    x.k = (int)(t % L.nzp);
-    const long long row = t / L.nzp;
-    x.j = (int)(row % L.ny);
-    x.i = (int)(row / L.ny);
+    long long row;
+    grid_coords(t, L.ny, L.nzp, x.i, x.j, x.k, row);
     x.m = t >> 1;
     x.col = (x.i + x.j + x.k) & 1;
     x.pad = x.k >= L.nz;
@@ -346,10 +344,9 @@ __global__ void unpack_t_kernel(double* out, const double* X0, const double* X1,
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long total = (long long)L.nx * L.ny * L.nz;
     if (t >= total) return;
-    const int k = (int)(t % L.nz);
-    const long long row = t / L.nz;
-    const int j = (int)(row % L.ny);
-    const int i = (int)(row / L.ny);
+    int i, j, k;
+    long long row;
+    grid_coords(t, L.ny, L.nz, i, j, k, row);
     const long long m = (row * L.nzp + k) >> 1;
     out[t] = ((i + j + k) & 1) ? X1[m] : X0[m];
 }

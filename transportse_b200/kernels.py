@@ -77,6 +77,12 @@ class Model:
         # FP64 solves' sweep kernel (args.sweep): 0 the bulk-copy staged
         # kernel where its stages fit, 1 plain loads; same cell values
         self.sweep = 0
+        # mixed-precision solves: the staged FP32 sweep's variant (chunk
+        # cells, ring stages, pipelines per block; 0 = the library's
+        # default), chosen per grid by transportse_b200.autotune; the last
+        # solve's variant as it ran
+        self.sweep_variant = (0, 0, 0)
+        self.last_variant = None
         # optional per-solve timing: list of (kind, start event, end event,
         # status) appended by the solver entry points when enabled
         self.timing = False
@@ -114,9 +120,11 @@ class Model:
                 self._solve_cluster(name, args_struct)
                 return
             opts = N.TseDcOptions(self.dc_cycle, getattr(self, "max_blocks", 0), int(self.timing))
+            opts.chunk, opts.ring, opts.pipes = self.sweep_variant
             rc = getattr(L, "tse_%s_dc" % name)(ct.byref(self.grid), ct.byref(args_struct),
                                                 ct.byref(opts), self._p(self.status),
                                                 self._p(self.ws), self.ws_bytes, self._stream())
+            self.last_variant = (opts.chunk, opts.ring, opts.pipes)
             if self.timing:
                 # per sweep-kernel timing of this solve: (kind, launches,
                 # red+black iterations, event ms)
