@@ -175,7 +175,10 @@ typedef struct TseDcOptions {
                                  as fit, up to 4) */
     int32_t pipes;            /* in/out: pipelines a block (1: two blocks per
                                  SM; else 2: one block per SM) */
-    int32_t reserved2;
+    int32_t graph_runs;       /* in/out, batched fused form, device-driven loop:
+                                 loop-body runs per graph launch before the host
+                                 relaunches the graph (<= 0: 4096); on return,
+                                 the graph launches the call made */
     int64_t active_cells;     /* in, batched fused form with the device-driven
                                  loop: cells (both colours, padding included)
                                  solving at once; the items wait in index order

@@ -118,7 +118,8 @@ def test_per_call_selectors_match_the_header_layout():
         assert T.sweep.offset == nptr * 8 + 7 * 8 + 8
         assert ct.sizeof(T) == nptr * 8 + 7 * 8 + 16
     assert N.TseDcOptions.host_loop.offset == 32 and N.TseDcOptions.loop_ms.offset == 40
-    assert N.TseDcOptions.chunk.offset == 48 and N.TseDcOptions.active_cells.offset == 64
+    assert N.TseDcOptions.chunk.offset == 48 and N.TseDcOptions.graph_runs.offset == 60
+    assert N.TseDcOptions.active_cells.offset == 64
     assert ct.sizeof(N.TseDcOptions) == 72
     L = N.lib()
     for name in ("tse_set_exact_sweep", "tse_set_batch_loop"):

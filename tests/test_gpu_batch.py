@@ -16,11 +16,12 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-6
 
 
-def _run_members(fns, device, cluster=0, host_loop=False, batch_cells=None):
+def _run_members(fns, device, cluster=0, host_loop=False, batch_cells=None, graph_runs=0):
     """Run fns[i](gate) on threads of their own, each on its own stream, all
     joined to one gate before any starts (so the first solves batch)."""
     from transportse_b200.batch import BatchGate
     gate = BatchGate(device, cluster=cluster, host_loop=host_loop, batch_cells=batch_cells)
+    gate.graph_runs = graph_runs
     out = [None] * len(fns)
     errs = []
     for _ in fns:
@@ -169,14 +170,18 @@ def test_device_loop_admitting_models_equals_host_loop(kw, cuda_device):
     ref, _ = _run_members([member(i) for i in range(len(SHAPES))], cuda_device, host_loop=True,
                           batch_cells=0)
     # 5,000 cells: the 28,800- and 11,781-cell models run alone, the rest in
-    # waves behind them
-    got, gate = _run_members([member(i) for i in range(len(SHAPES))], cuda_device,
-                             batch_cells=5000)
-    st = gate.stats()
-    assert st["launches"]["compute_P"] == 1 and st["solves"]["compute_P"] == len(SHAPES)
-    for i, (a, b) in enumerate(zip(got, ref)):
-        assert (a[0], a[1], a[4], a[5]) == (b[0], b[1], b[4], b[5]), SHAPES[i]
-        assert numpy.array_equal(a[2], b[2]), SHAPES[i]
+    # waves behind them; then the same with the graph relaunched by the host
+    # every 3 loop-body runs (TseDcOptions.graph_runs), which a solve of more
+    # than 4,096 sweep launches would do
+    for runs in (0, 3):
+        got, gate = _run_members([member(i) for i in range(len(SHAPES))], cuda_device,
+                                 batch_cells=5000, graph_runs=runs)
+        st = gate.stats()
+        assert st["launches"]["compute_P"] == 1 and st["solves"]["compute_P"] == len(SHAPES)
+        assert (st["graph_launches"] > 3) == (runs == 3), st["graph_launches"]
+        for i, (a, b) in enumerate(zip(got, ref)):
+            assert (a[0], a[1], a[4], a[5]) == (b[0], b[1], b[4], b[5]), (SHAPES[i], runs)
+            assert numpy.array_equal(a[2], b[2]), (SHAPES[i], runs)
 
 
 def test_batched_halving_and_stop_follow_the_reference(cuda_device):

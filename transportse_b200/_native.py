@@ -80,7 +80,7 @@ class TseDcOptions(ct.Structure):
                 ("sweep_launches", ct.c_int32), ("sweep_iterations", ct.c_int64),
                 ("sweep_ms", ct.c_double), ("host_loop", ct.c_int32), ("reserved", ct.c_int32),
                 ("loop_ms", ct.c_double), ("chunk", ct.c_int32), ("ring", ct.c_int32),
-                ("pipes", ct.c_int32), ("reserved2", ct.c_int32), ("active_cells", ct.c_int64)]
+                ("pipes", ct.c_int32), ("graph_runs", ct.c_int32), ("active_cells", ct.c_int64)]
 
 
 def _batch_item(args_type):

@@ -98,6 +98,10 @@ class BatchGate:
         self.cluster = int(cluster)
         self.eager = bool(eager)
         self.host_loop = bool(host_loop)
+        # device-driven loop: body runs per graph launch (0: the library's
+        # 4096); graph launches made so far, in the statistics
+        self.graph_runs = 0
+        self.graph_launches = 0
         if batch_cells is None:
             batch_cells = default_batch_cells(self.device)
         self.batch_cells = int(batch_cells)
@@ -257,6 +261,7 @@ class BatchGate:
         opts = N.TseDcOptions(cycle, self.cluster, 1)
         opts.host_loop = int(self.host_loop)
         opts.active_cells = max(0, self.batch_cells)
+        opts.graph_runs = int(self.graph_runs)
         rc = getattr(L, "tse_%s_dc_batch" % name)(items, len(rs), ct.byref(opts),
                                                   ct.c_void_p(ws.data_ptr()), ws.numel(),
                                                   ct.c_void_p(bs.cuda_stream))
@@ -267,6 +272,8 @@ class BatchGate:
         self.sweeps[name][1] += opts.sweep_iterations
         self.sweeps[name][2] += opts.sweep_ms
         self.sweeps[name][3] += opts.loop_ms
+        if not self.host_loop and self.cluster <= 0:
+            self.graph_launches += opts.graph_runs
 
     def stats(self):
         # sweeps: the fused sweep kernel's launches, the global iterations
@@ -274,6 +281,7 @@ class BatchGate:
         # them (sweeps, events, x += d, residuals)
         return {"launches": dict(self.launches), "solves": dict(self.solves),
                 "call_s": round(self.call_s, 3), "gap_s": round(self.gap_s, 3),
+                "graph_launches": self.graph_launches,
                 "sweeps": {k: {"launches": v[0], "iterations": v[1], "ms": round(v[2], 3),
                                "loop_ms": round(v[3], 3)}
                            for k, v in self.sweeps.items()}}

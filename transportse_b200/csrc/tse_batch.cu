@@ -29,6 +29,8 @@
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <mutex>
+#include <type_traits>
 #include <cooperative_groups.h>
 
 #include "tse_dc.cuh"
@@ -449,6 +451,17 @@ __device__ void fused_decide(const FusedItem& I, int g, int num_it, bool check, 
     if (ev != EV_NONE) atomicExch(any_event, 1);
 }
 
+// What a consumer group needs of a staged chunk besides its copied arrays,
+// written by the producer into the stage's header before the copies are
+// issued (the stage's full barrier publishes it with them), so consumers
+// read no table or model record from global memory
+struct ChunkHdr {
+    long long m0, SX, Nc;
+    float* out;
+    int H;
+    float sor;
+};
+
 template <int RING, int PIPES>
 __device__ __forceinline__ void fused_sweep_body(const FusedArgs& A, const TmaStage& T) {
     constexpr int kPipes = PIPES;
@@ -457,6 +470,7 @@ __device__ __forceinline__ void fused_sweep_body(const FusedArgs& A, const TmaSt
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ __align__(8) uint64_t full[RING * PIPES];
     __shared__ __align__(8) uint64_t empty[RING * PIPES];
+    __shared__ ChunkHdr hdr[RING * PIPES];
     __shared__ double sh[kFusedThreads / 32];
     __shared__ int s_err;
     const unsigned nb = gridDim.x, b = blockIdx.x;
@@ -494,22 +508,52 @@ __device__ __forceinline__ void fused_sweep_body(const FusedArgs& A, const TmaSt
         const bool last = g == A.g_max;
         for (int col = 0; col < 2 && ok; ++col) {
             if (producer) {
-                if (lane == 0) {
-                    fence_proxy_async();
-                    for (long long j = 0; j < pmine; ++j, ++issued) {
-                        const unsigned s = ring0 + issued % RING;
-                        if (issued >= (unsigned)RING &&
-                            !mbar_wait_flag(&empty[s], (issued / RING - 1) & 1u, err))
+                // the warp fetches the table entries of its next 32 chunks at
+                // once (one memory round trip per 32 chunks, not per chunk);
+                // lane 0 takes each from its lane, reads the chunk's model
+                // record (cached after its first chunk), writes the consumers'
+                // header and issues the copies
+                if (lane == 0) fence_proxy_async();
+                bool pok = true;
+                for (long long j0 = 0; j0 < pmine && pok; j0 += 32) {
+                    FusedChunk mine_ch = {0, 0, 0};
+                    if (j0 + lane < pmine) mine_ch = A.chunks[b + (pipe + (j0 + lane) * kPipes) * nb];
+                    const int nj = (int)((pmine - j0) < 32 ? (pmine - j0) : 32);
+                    for (int t = 0; t < nj; ++t) {
+                        const long long m0 = __shfl_sync(0xffffffffu, mine_ch.m0, t);
+                        const int item = __shfl_sync(0xffffffffu, mine_ch.item, t);
+                        int okw = 1;
+                        if (lane == 0) {
+                            const unsigned s = ring0 + issued % RING;
+                            if (issued >= (unsigned)RING &&
+                                !mbar_wait_flag(&empty[s], (issued / RING - 1) & 1u, err)) {
+                                okw = 0;
+                            } else {
+                                const DcCtl& c = A.items[item].c;
+                                const long long cnt = (c.Ncal - m0) < C ? (c.Ncal - m0) : C;
+                                unsigned char* stg = smem + (size_t)s * T.bytes;
+                                ChunkHdr h;
+                                h.m0 = m0;
+                                h.SX = c.L.SX;
+                                h.Nc = c.L.Nc;
+                                h.out = c.D[col] + m0;
+                                h.H = c.L.H;
+                                h.sor = c.sor;
+                                hdr[s] = h;
+                                tma_issue_own_n(c.Ncal, T, stg, &full[s], c.K[col], c.D[col], c.mask[col], m0,
+                                                cnt);
+                                tma_issue_windows_n(h.SX, h.H, T, stg, &full[s], c.D[1 - col], m0);
+                                ++issued;
+                            }
+                        }
+                        if (!__shfl_sync(0xffffffffu, okw, 0)) {
+                            pok = false;
                             break;
-                        const FusedChunk ch = A.chunks[b + (pipe + j * kPipes) * nb];
-                        const DcCtl& c = A.items[ch.item].c;
-                        const long long cnt = (c.Ncal - ch.m0) < C ? (c.Ncal - ch.m0) : C;
-                        unsigned char* stg = smem + (size_t)s * T.bytes;
-                        tma_issue_own(c, T, stg, &full[s], c.K[col], c.D[col], c.mask[col], ch.m0, cnt);
-                        tma_issue_windows(c, T, stg, &full[s], c.D[1 - col], ch.m0);
+                        }
                     }
                 }
-                __syncwarp();
+                // lane 0 counted the copies it issued; the other lanes follow
+                issued = __shfl_sync(0xffffffffu, issued, 0);
             } else {
                 for (long long j = grank; j < pmine; j += kGroupsPerPipe) {
                     const unsigned u = uses + (unsigned)j;
@@ -522,12 +566,11 @@ __device__ __forceinline__ void fused_sweep_body(const FusedArgs& A, const TmaSt
                     mbar_try_wait(&full[s], (u / RING) & 1u);
                     const unsigned char* stg = smem + (size_t)s * T.bytes;
                     const long long q = b + (pipe + j * kPipes) * nb;
-                    const FusedChunk ch = A.chunks[q];
-                    const DcCtl& c = A.items[ch.item].c;
-                    const long long m0 = ch.m0, SX = c.L.SX;
-                    const int H = c.L.H;
-                    const float sor = c.sor;
-                    const int nval = (int)((c.L.Nc - m0) < C ? (c.L.Nc - m0) : C);
+                    const ChunkHdr h = hdr[s];
+                    const long long m0 = h.m0, SX = h.SX;
+                    const int H = h.H;
+                    const float sor = h.sor;
+                    const int nval = (int)((h.Nc - m0) < C ? (h.Nc - m0) : C);
                     const int oz = (int)(m0 - ((m0 - H - 1) & ~3LL));
                     const int oxp = (int)(m0 + SX - ((m0 + SX) & ~3LL));
                     const int oxm = (int)(m0 - SX - ((m0 - SX) & ~3LL));
@@ -538,7 +581,7 @@ __device__ __forceinline__ void fused_sweep_body(const FusedArgs& A, const TmaSt
                     const float* wz = reinterpret_cast<const float*>(stg + T.wz);
                     const float* wxp = reinterpret_cast<const float*>(stg + T.wxp);
                     const float* wxm = reinterpret_cast<const float*>(stg + T.wxm);
-                    float* out = c.D[col] + m0;
+                    float* out = h.out;
                     float d2 = 0.0f, dd = 0.0f;
 #pragma unroll
                     for (int r = 0; r < kTmaCellsPerThread; ++r) {
@@ -915,6 +958,8 @@ struct FusedCtl {
     long long resid_total;   // residual blocks of the current body run, all models
     unsigned long long sweep_ns;   // summed duration of the sweep launches
     long long budget;        // cells (both colours) active at once; 0: every model
+    int max_runs;            // loop-body runs per graph launch
+    int pad;
 };
 
 __device__ void fused_add_sweep_ns(FusedCtl* ctl, unsigned long long ns) { ctl->sweep_ns += ns; }
@@ -1168,7 +1213,7 @@ __global__ void __launch_bounds__(kPlanThreads) fused_events_kernel(FusedCtl* ct
         ctl->resid_total = s_base;
         if (failed) ctl->failed = 1;
         ctl->nactive = s_active;
-        cudaGraphSetConditional(cond, (s_active > 0 && !failed && ctl->runs < kGraphMaxRuns) ? 1u : 0u);
+        cudaGraphSetConditional(cond, (s_active > 0 && !failed && ctl->runs < ctl->max_runs) ? 1u : 0u);
     }
 }
 
@@ -1247,6 +1292,85 @@ static size_t fused_loop_bytes(int n) {
            align256(sizeof(FusedArgs)) + align256(sizeof(FusedCtl)) + align256(form * n);
 }
 
+// Instantiated device-loop graphs, kept across calls.  A graph's nodes hold
+// the addresses it carves from the batch workspace, the launch shapes and
+// the stage layout, which the key fixes (device, form, workspace address,
+// model count, total cells, tallest column, ring length); everything that
+// varies between calls -- the models, their state, their arguments -- goes in
+// through the workspace before the launch.  Slots are handed out one call at
+// a time (a slot in use is neither shared nor evicted); a call that finds
+// every slot busy builds its own graph and destroys it at the end.  The cache
+// is kept until the process exits (a device reset is not supported).
+struct GraphKey {
+    int dev, form;
+    const void* ws;
+    int n;
+    long long cells;
+    int Hmax, ring;
+    bool operator==(const GraphKey& o) const {
+        return dev == o.dev && form == o.form && ws == o.ws && n == o.n && cells == o.cells &&
+               Hmax == o.Hmax && ring == o.ring;
+    }
+};
+struct GraphSlot {
+    GraphKey key;
+    cudaGraph_t graph;
+    cudaGraphExec_t exec;
+    bool busy;
+    unsigned long long used;   // last use, for eviction
+};
+constexpr int kGraphSlots = 32;
+static std::mutex g_graph_mu;
+static GraphSlot g_graph_slots[kGraphSlots];
+static unsigned long long g_graph_clock = 0;
+
+// the cached graph of `key` (slot->exec set), or a slot reserved for it
+// (exec null: the caller builds and hands the graph over at release), or
+// null when every slot is busy
+static GraphSlot* graph_cache_acquire(const GraphKey& key) {
+    std::lock_guard<std::mutex> lk(g_graph_mu);
+    GraphSlot* victim = nullptr;
+    for (auto& s : g_graph_slots) {
+        if (s.exec && s.key == key && !s.busy) {
+            s.busy = true;
+            s.used = ++g_graph_clock;
+            return &s;
+        }
+    }
+    for (auto& s : g_graph_slots) {
+        if (s.busy) continue;
+        if (!s.exec) { victim = &s; break; }
+        if (!victim || s.used < victim->used) victim = &s;
+    }
+    if (!victim) return nullptr;
+    if (victim->exec) {
+        cudaGraphExecDestroy(victim->exec);
+        cudaGraphDestroy(victim->graph);
+        victim->exec = nullptr;
+        victim->graph = nullptr;
+    }
+    victim->key = key;
+    victim->busy = true;
+    victim->used = ++g_graph_clock;
+    return victim;
+}
+
+// end of a call: a graph built for a reserved slot goes into it; without a
+// slot the graph is destroyed
+static void graph_cache_release(GraphSlot* slot, cudaGraph_t graph, cudaGraphExec_t exec) {
+    std::lock_guard<std::mutex> lk(g_graph_mu);
+    if (!slot) {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        return;
+    }
+    if (!slot->exec && exec) {
+        slot->exec = exec;
+        slot->graph = graph;
+    }
+    slot->busy = false;
+}
+
 // batch solves run by each loop since the library was loaded
 std::atomic<long long> g_graph_solves{0}, g_host_solves{0};
 
@@ -1322,58 +1446,74 @@ static int run_fused_graph(std::vector<BatchItem<Form>>& v, TseDcOptions* opts, 
     if (nb > (long long)nch_max) nb = (long long)nch_max;
     const unsigned grid_small = (unsigned)(4 * sms), grid_big = (unsigned)(8 * sms);
 
-    // the graph: one WHILE node, its body captured from the stream
+    // the graph: one WHILE node, its body captured from the stream.  Its
+    // nodes hold only workspace addresses, launch shapes and the stage
+    // layout, all fixed by the key, so a later call with the same key reuses
+    // the instantiated graph (the models' data go in through the workspace)
+    const GraphKey key{dev, std::is_same<Form, PressureForm>::value ? 0 : 1, d_ws, n, cells, Hmax, ring};
+    GraphSlot* slot = graph_cache_acquire(key);
     cudaGraph_t graph = nullptr, body = nullptr;
-    cudaGraphExec_t exec = nullptr;
+    cudaGraphExec_t exec = slot ? slot->exec : nullptr;
     cudaGraphConditionalHandle cond;
-    bool built = cudaGraphCreate(&graph, 0) == cudaSuccess &&
-                 cudaGraphConditionalHandleCreate(&cond, graph, 1, cudaGraphCondAssignDefault) == cudaSuccess;
-    if (built) {
-        cudaGraphNodeParams cp = {};
-        cp.type = cudaGraphNodeTypeConditional;
-        cp.conditional.handle = cond;
-        cp.conditional.type = cudaGraphCondTypeWhile;
-        cp.conditional.size = 1;
-        cudaGraphNode_t node;
-        built = cudaGraphAddNode(&node, graph, nullptr, 0, &cp) == cudaSuccess;
-        if (built) body = cp.conditional.phGraph_out[0];
-    }
-    if (built)
-        built = cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) ==
-                cudaSuccess;
-    if (built) {
-        fused_plan_kernel<<<1, kPlanThreads, 0, stream>>>(d_ctl, d_models, d_items, d_idx, d_args, d_chunks,
-                                                          d_cpart, d_any, d_bar);
-        fused_fill_kernel<<<grid_small, kBlock, 0, stream>>>(d_args, d_chunks);
-        cudaLaunchConfig_t lc = {};
-        lc.gridDim = dim3((unsigned)nb);
-        lc.blockDim = dim3((unsigned)fused_threads);
-        lc.dynamicSmemBytes = smem;
-        lc.stream = stream;
-        cudaLaunchAttribute at[1];
-        at[0].id = cudaLaunchAttributeCooperative;
-        at[0].val.cooperative = 1;
-        lc.attrs = at;
-        lc.numAttrs = 1;
-        const FusedArgs* a_ptr = d_args;
-        FusedCtl* c_ptr = d_ctl;
-        void* kargs[] = {(void*)&a_ptr, (void*)&T, (void*)&c_ptr};
-        const cudaError_t le = cudaLaunchKernelExC(&lc, kernel, kargs);
-        fused_events_kernel<<<1, kPlanThreads, 0, stream>>>(d_ctl, d_models, d_args, d_idx, d_act, d_rstart,
-                                                            cond);
-        fused_update_kernel<Form><<<grid_big, kBlock, 0, stream>>>(d_args, d_forms, d_idx, d_act);
-        fused_residual_kernel<Form><<<grid_big, kBlock, 0, stream>>>(d_args, d_forms, d_idx, d_rstart, d_ctl);
-        fused_x2_kernel<<<grid_small, kBlock, 0, stream>>>(d_args, d_act);
-        const cudaError_t ce = cudaStreamEndCapture(stream, &body);
-        built = le == cudaSuccess && ce == cudaSuccess && cudaGetLastError() == cudaSuccess;
-    }
-    if (built) built = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+    bool built = exec != nullptr;
     if (!built) {
-        cudaGetLastError();
-        if (exec) cudaGraphExecDestroy(exec);
-        if (graph) cudaGraphDestroy(graph);
-        return 1;
+        built = cudaGraphCreate(&graph, 0) == cudaSuccess &&
+                cudaGraphConditionalHandleCreate(&cond, graph, 1, cudaGraphCondAssignDefault) == cudaSuccess;
+        if (built) {
+            cudaGraphNodeParams cp = {};
+            cp.type = cudaGraphNodeTypeConditional;
+            cp.conditional.handle = cond;
+            cp.conditional.type = cudaGraphCondTypeWhile;
+            cp.conditional.size = 1;
+            cudaGraphNode_t node;
+            built = cudaGraphAddNode(&node, graph, nullptr, 0, &cp) == cudaSuccess;
+            if (built) body = cp.conditional.phGraph_out[0];
+        }
+        if (built)
+            built = cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) ==
+                    cudaSuccess;
+        if (built) {
+            fused_plan_kernel<<<1, kPlanThreads, 0, stream>>>(d_ctl, d_models, d_items, d_idx, d_args, d_chunks,
+                                                              d_cpart, d_any, d_bar);
+            fused_fill_kernel<<<grid_small, kBlock, 0, stream>>>(d_args, d_chunks);
+            cudaLaunchConfig_t lc = {};
+            lc.gridDim = dim3((unsigned)nb);
+            lc.blockDim = dim3((unsigned)fused_threads);
+            lc.dynamicSmemBytes = smem;
+            lc.stream = stream;
+            cudaLaunchAttribute at[1];
+            at[0].id = cudaLaunchAttributeCooperative;
+            at[0].val.cooperative = 1;
+            lc.attrs = at;
+            lc.numAttrs = 1;
+            const FusedArgs* a_ptr = d_args;
+            FusedCtl* c_ptr = d_ctl;
+            void* kargs[] = {(void*)&a_ptr, (void*)&T, (void*)&c_ptr};
+            const cudaError_t le = cudaLaunchKernelExC(&lc, kernel, kargs);
+            fused_events_kernel<<<1, kPlanThreads, 0, stream>>>(d_ctl, d_models, d_args, d_idx, d_act, d_rstart,
+                                                                cond);
+            fused_update_kernel<Form><<<grid_big, kBlock, 0, stream>>>(d_args, d_forms, d_idx, d_act);
+            fused_residual_kernel<Form><<<grid_big, kBlock, 0, stream>>>(d_args, d_forms, d_idx, d_rstart, d_ctl);
+            fused_x2_kernel<<<grid_small, kBlock, 0, stream>>>(d_args, d_act);
+            const cudaError_t ce = cudaStreamEndCapture(stream, &body);
+            built = le == cudaSuccess && ce == cudaSuccess && cudaGetLastError() == cudaSuccess;
+        }
+        if (built) built = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+        if (!built) {
+            cudaGetLastError();
+            if (exec) cudaGraphExecDestroy(exec);
+            if (graph) cudaGraphDestroy(graph);
+            graph_cache_release(slot, nullptr, nullptr);
+            return 1;
+        }
     }
+    // the graph goes back to the cache (or is destroyed) when the call ends
+    struct Release {
+        GraphSlot* slot;
+        cudaGraph_t graph;
+        cudaGraphExec_t exec;
+        ~Release() { graph_cache_release(slot, graph, exec); }
+    } release{slot, graph, exec};
 
     // every model: state, scaled records, first residual (as run_fused)
     int rc = TSE_OK;
@@ -1399,6 +1539,7 @@ static int run_fused_graph(std::vector<BatchItem<Form>>& v, TseDcOptions* opts, 
     hc.n = n;
     hc.nactive = n;
     hc.budget = budget;
+    hc.max_runs = (opts && opts->graph_runs > 0) ? opts->graph_runs : kGraphMaxRuns;
     // pageable sources: staged before the calls return
     if (rc == TSE_OK &&
         (cudaMemcpyAsync(d_models, hm.data(), sizeof(FusedModel) * n, cudaMemcpyHostToDevice, stream) !=
@@ -1413,8 +1554,10 @@ static int run_fused_graph(std::vector<BatchItem<Form>>& v, TseDcOptions* opts, 
         rc = TSE_ERR_LAUNCH;
     if (rc == TSE_OK && timing) cudaEventRecord(ev0, stream);
     // graph launches until every model has finished: one, unless a solve needs
-    // more than kGraphMaxRuns sweep launches
+    // more than max_runs sweep launches
+    int launches = 0;
     for (int launch = 0; rc == TSE_OK; ++launch) {
+        ++launches;
         if (cudaGraphLaunch(exec, stream) != cudaSuccess ||
             cudaMemcpyAsync(&hc, d_ctl, sizeof(FusedCtl), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
             cudaStreamSynchronize(stream) != cudaSuccess) {
@@ -1442,8 +1585,7 @@ static int run_fused_graph(std::vector<BatchItem<Form>>& v, TseDcOptions* opts, 
         cudaEventDestroy(ev0);
         cudaEventDestroy(ev1);
     }
-    cudaGraphExecDestroy(exec);
-    cudaGraphDestroy(graph);
+    if (opts) opts->graph_runs = launches;
     g_graph_solves.fetch_add(1);
     // status records and results of every model
     for (auto& it : v) {

@@ -250,10 +250,9 @@ __host__ __device__ inline TmaStage tma_stage(int H, int C = kTmaChunk) {
 // transaction count without arriving.  The second part (the three windows of
 // the other colour, which other blocks have just written) is issued after the
 // barrier and carries the stage's single arrival.
-__device__ __forceinline__ void tma_issue_own(const DcCtl& c, const TmaStage& T, unsigned char* stage,
-                                              uint64_t* bar, const float* Kc, const float* dw,
-                                              const uint8_t* msk, long long m0, long long cnt) {
-    const long long N = c.Ncal;
+__device__ __forceinline__ void tma_issue_own_n(long long N, const TmaStage& T, unsigned char* stage,
+                                                uint64_t* bar, const float* Kc, const float* dw,
+                                                const uint8_t* msk, long long m0, long long cnt) {
     const unsigned b_rec = (unsigned)(24 * cnt), b_rp = (unsigned)(4 * cnt), b_msk = (unsigned)cnt,
                    b_dw = (unsigned)(4 * cnt);
     const uint64_t first = l2_evict_first(), last = l2_evict_last();
@@ -262,13 +261,17 @@ __device__ __forceinline__ void tma_issue_own(const DcCtl& c, const TmaStage& T,
     bulk_g2s_hint(stage + T.rp, Kc + 6 * N + m0, b_rp, bar, first);
     bulk_g2s_hint(stage + T.msk, msk + m0, b_msk, bar, first);
     bulk_g2s_hint(stage + T.dw, dw + m0, b_dw, bar, last);
-    (void)N;
 }
 
-__device__ __forceinline__ void tma_issue_windows(const DcCtl& c, const TmaStage& T, unsigned char* stage,
-                                                  uint64_t* bar, const float* dq, long long m0) {
-    const long long SX = c.L.SX;
-    const int H = c.L.H;
+__device__ __forceinline__ void tma_issue_own(const DcCtl& c, const TmaStage& T, unsigned char* stage,
+                                              uint64_t* bar, const float* Kc, const float* dw,
+                                              const uint8_t* msk, long long m0, long long cnt) {
+    tma_issue_own_n(c.Ncal, T, stage, bar, Kc, dw, msk, m0, cnt);
+}
+
+__device__ __forceinline__ void tma_issue_windows_n(long long SX, int H, const TmaStage& T,
+                                                    unsigned char* stage, uint64_t* bar, const float* dq,
+                                                    long long m0) {
     const long long zs = (m0 - H - 1) & ~3LL;
     const long long xps = (m0 + SX) & ~3LL;
     const long long xms = (m0 - SX) & ~3LL;
@@ -280,6 +283,11 @@ __device__ __forceinline__ void tma_issue_windows(const DcCtl& c, const TmaStage
     bulk_g2s_hint(stage + T.wz, dq + zs, b_z, bar, last);
     bulk_g2s_hint(stage + T.wxp, dq + xps, b_x, bar, last);
     bulk_g2s_hint(stage + T.wxm, dq + xms, b_x, bar, last);
+}
+
+__device__ __forceinline__ void tma_issue_windows(const DcCtl& c, const TmaStage& T, unsigned char* stage,
+                                                  uint64_t* bar, const float* dq, long long m0) {
+    tma_issue_windows_n(c.L.SX, c.L.H, T, stage, bar, dq, m0);
 }
 
 // Roles: warps 0-7 consume, in two groups of four warps; group g computes the
