@@ -1013,15 +1013,19 @@ __device__ V block_inclusive_scan(V v, V* sh, V* total) {
 // share of the GPU to the next ones instead of leaving it idle until the
 // slowest model of the batch is done.  An admitted model counts its own
 // iterations from 0 (its state record is its solve's from the start), so
-// its iterations, checks and decisions are those of its solve alone.
+// its iterations, checks and decisions are those of its solve alone.  Under
+// the pressure schedule (checks every 10th of a model's own iterations past
+// its 50th) models join only on multiples of 10 of the loop's count -- a
+// launch ends there while models wait and room is free -- so the running
+// models share one check phase and most iterations need no check at all.
 __global__ void __launch_bounds__(kPlanThreads) fused_plan_kernel(const FusedCtl* ctl, FusedModel* models,
                                                                   FusedItem* items, int* idx, FusedArgs* args,
                                                                   FusedChunk* chunks, double2* cpart,
                                                                   int* any_event, GridBarrier* bar) {
     __shared__ long long sh_ll[32];
     __shared__ int sh_i[32];
-    __shared__ int s_gmax, s_base_k, s_young, s_mask;
-    __shared__ long long s_base_ch, s_active_cells, s_base_w;
+    __shared__ int s_gmax, s_base_k, s_young, s_mask, s_cap;
+    __shared__ long long s_base_ch, s_active_cells, s_base_w, s_waiting_cells;
     const int n = ctl->n;
     if (threadIdx.x == 0) {
         s_gmax = 1 << 30;
@@ -1031,22 +1035,35 @@ __global__ void __launch_bounds__(kPlanThreads) fused_plan_kernel(const FusedCtl
         s_base_w = 0;
         s_young = 1 << 30;
         s_mask = 0;
+        s_cap = 1 << 30;
+        s_waiting_cells = 0;
     }
     __syncthreads();
     if (ctl->budget > 0) {
-        // cells of the active models
+        // cells of the active models and of the waiting ones
         for (int base = 0; base < n; base += kPlanThreads) {
             const int i = base + threadIdx.x;
             const long long cells = (i < n && models[i].active) ? 2 * models[i].c.L.Nc : 0;
-            long long tot;
+            const long long wcells = (i < n && models[i].waiting) ? 2 * models[i].c.L.Nc : 0;
+            long long tot, wtot;
             block_inclusive_scan<long long>(cells, sh_ll, &tot);
-            if (threadIdx.x == 0) s_active_cells += tot;
+            block_inclusive_scan<long long>(wcells, sh_ll, &wtot);
+            if (threadIdx.x == 0) {
+                s_active_cells += tot;
+                s_waiting_cells += wtot;
+            }
             __syncthreads();
         }
-        // waiting models in index order, while they fit
+        // waiting models in index order, while they fit -- under the pressure
+        // schedule on multiples of 10 of the loop's count (any time when no
+        // model runs); between them the launch ends at the next multiple
         const long long room = ctl->budget - s_active_cells;
         const bool none = s_active_cells == 0;
-        for (int base = 0; base < n; base += kPlanThreads) {
+        const int phase = ctl->num_it % 10;
+        const bool sched = models[0].c.pressure_schedule != 0;
+        const bool admit_now = none || !sched || phase == 0;
+        if (!admit_now && s_waiting_cells > 0 && room > 0 && threadIdx.x == 0) s_cap = 10 - phase;
+        for (int base = 0; base < n && admit_now; base += kPlanThreads) {
             const int i = base + threadIdx.x;
             const bool w = i < n && models[i].waiting;
             const long long cells = w ? 2 * models[i].c.L.Nc : 0;
@@ -1111,7 +1128,8 @@ __global__ void __launch_bounds__(kPlanThreads) fused_plan_kernel(const FusedCtl
         A.cpart = cpart;
         A.any_event = any_event;
         A.bar = bar;
-        A.g_max = s_gmax < 1 ? 1 : s_gmax;
+        const int gm = s_gmax < s_cap ? s_gmax : s_cap;
+        A.g_max = gm < 1 ? 1 : gm;
         A.num_it0 = ctl->num_it;
         A.pressure_schedule = s_base_k > 0 ? items[0].c.pressure_schedule : 0;
         A.young = s_young;
