@@ -1,9 +1,10 @@
 """The GPU driver against the oracle at sizes the committed fixtures do not
 reach: the bottom-heated reservoir generator at 64 x 64 x 32 (131,072 cells;
 geometric spacing, random-field permeability, two species plus heat, linear
-EOS, SIA) and the sloped model at 32^3 over 10 steps (5 degree slope,
+EOS, SIA), the sloped model at 32^3 over 10 steps (5 degree slope,
 anisotropic permeability, three species with dispersivity, Smolarkiewicz
-correction, NLTE heat).
+correction, NLTE heat), an ensemble member at 48 x 40 x 36 and a serving
+request at 48^3.
 
 The oracle is the bit-exact C restatement of the reference (pinned to the
 reference's own runs by tests/test_oracle_golden.py), so these runs stand in
@@ -27,6 +28,12 @@ CASES = {
                            (1, 4), ("P", "C", "T", "qx", "qy", "qz", "rho_f")),
     "sloped_32x32x32": ("sloped_3d", {"nx": 32, "ny": 32, "nz": 32, "seed": 5}, 10,
                         (1, 5, 10), ("P", "C", "T", "qx", "qy", "qz")),
+    # an ensemble member and a serving request from the middle of their
+    # configs' size ranges (32-128 per axis; cubic 16-192)
+    "ensemble_member_48x40x36": ("ensemble_member", {"seed": 1007, "shape": (48, 40, 36)}, 4,
+                                 (1, 4), ("P", "C", "T", "qx", "qy", "qz")),
+    "serving_request_48": ("serving_request", {"seed": 5003, "n": 48}, 4, (1, 4),
+                           ("P", "C", "T", "qx", "qy", "qz")),
 }
 
 
@@ -110,3 +117,34 @@ def test_dc_driver_matches_oracle_at_size(name, cuda_device):
     for k in ("numitC", "numitT"):
         a, b = s[k][-1], ref_s[k][-1]
         assert abs(a - b) <= 0.25 * b + 10, (k, a, b)
+
+
+@pytest.mark.parametrize("builder,shape,steps", [
+    ("reservoir_3d", (256, 256, 128), 2),
+    ("sloped_3d", (256, 256, 128), 2)])
+def test_dc_matches_fp64_at_benchmark_size(builder, shape, steps, cuda_device):
+    """At the benchmark's own size -- the 256 x 256 x 128 reservoir, and the
+    sloped model with every feature of the large-model config (slope,
+    anisotropy, three species with dispersivity, Smolarkiewicz correction,
+    NLTE heat, SIA) at the same size -- the FP32 + defect-correction form
+    against the FP64 form (the reference's arithmetic, pinned to the
+    reference at the sizes above): every field, the Darcy fluxes and the
+    pressure change within 1e-6; the same time and pressure iteration count
+    to 2 %."""
+    from transportse_b200 import workloads
+    from transportse_b200.driver import Simulation
+    cfg = getattr(workloads, builder)(*shape)
+    P0 = numpy.asarray(cfg.P)
+    out = {}
+    for prec in ("fp64", "fp32dc"):
+        sim = Simulation(getattr(workloads, builder)(*shape), device=cuda_device, precision=prec)
+        sim.run(max_steps=steps)
+        out[prec] = ({n: sim.field(n) for n in ("P", "C", "T", "qx", "qy", "qz", "rho_f")},
+                     dict(sim.counters), sim.t_sim)
+        del sim
+    (f64, c64, t64), (f32, c32, t32) = out["fp64"], out["fp32dc"]
+    assert abs(t32 - t64) <= 1e-6 * t64
+    assert abs(c32["P"] - c64["P"]) <= max(10, 0.02 * c64["P"]), (c32, c64)
+    for n, ref in f64.items():
+        assert rel_err(f32[n], ref) <= 1e-6, (n, rel_err(f32[n], ref))
+    assert dynamic_pressure_err(f32["P"], f64["P"], P0) <= 1e-6

@@ -51,11 +51,12 @@ class _Request:
 
 
 def default_batch_cells(device):
-    """The fused form's default sub-batch budget: 12M cells on a B200 (126 MB
-    of L2), i.e. L2 bytes / 10.5.  Measured on the 512-model ensemble (axes
-    log-uniform 32-128, 164M cells, 3 steps): 96.0 G cell-updates/s as one
-    batch, 90.3 at 4M-cell sub-batches, 103.4 at 8M, 104.3 at 16M, 95.2 at
-    32M."""
+    """The fused form's default cell budget: 12M cells on a B200 (126 MB of
+    L2), i.e. L2 bytes / 10.5.  Measured on the 512-model ensemble (axes
+    log-uniform 32-128, 164M cells, 3 steps): models admitted into the
+    running loop under 6M / 9M / 12M / 18M cells 104.4 / 107.4 / 109.3 /
+    102.8 G cell-updates/s; as size-sorted sub-batches (the host loop's form)
+    4M / 8M / 16M / 32M cells 90.3 / 103.4 / 104.3 / 95.2, one batch 96.0."""
     device = torch.device(device)
     if device.type != "cuda":
         return 0
