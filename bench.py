@@ -657,7 +657,7 @@ def main():
     tune = None
     if not a.no_autotune:
         # the staged sweep's chunk / ring / pipelines for this grid, timed on
-        # its own pressure solve (results do not depend on the choice)
+        # its own pressure solve (every variant makes the same cell updates)
         from transportse_b200 import autotune
         tune = autotune.tune_sweep(sim)
     for _ in range(a.warmup):

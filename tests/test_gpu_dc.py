@@ -122,3 +122,51 @@ def test_dc_driver_matches_reference_course_models(name, cuda_device, tmp_path):
             assert rel_err(got[k], fx[k]) <= TOL, (k, rel_err(got[k], fx[k]))
             if k.startswith("P@"):
                 assert dynamic_pressure_err(got[k], fx[k], P0) <= TOL, k
+
+
+def test_sweep_variants_give_identical_results(cuda_device):
+    """The staged sweep's compiled variants (chunk of 256/512/1024 cells, ring
+    of 2-4 stages, 1 or 2 pipelines) only reschedule the same cell updates:
+    a mixed-precision pressure solve and a species solve give the same fields,
+    iteration counts and dt bit for bit under each (the check sums are
+    grouped by chunk, but no norm of these solves lies within rounding of its
+    tolerance), and the call reports the variant that ran."""
+    from transportse_b200 import workloads
+    shape = (40, 36, 50)
+    rng = numpy.random.default_rng(17)
+    cfg = workloads.base_config("var", *shape, rng.uniform(0.5, 2, shape[0]),
+                                rng.uniform(0.5, 2, shape[1]), rng.uniform(0.5, 2, shape[2]))
+    cfg.beta = 3.0
+    cfg.c_r[:] = 1e-10
+    K = 1e-12 * numpy.exp(rng.standard_normal(shape))
+    pargs = (4.5e-10 * numpy.ones(shape), rng.uniform(8e-4, 1.2e-3, shape),
+             rng.uniform(995, 1150, shape), rng.uniform(0.05, 0.3, shape), K, K, 0.3 * K)
+    z = numpy.zeros(shape)
+    P = workloads.hydrostatic(cfg) + rng.uniform(-300, 300, shape)
+    BP = numpy.zeros(shape)
+    BP[:, :, -1] = 1
+    WP = numpy.where(rng.uniform(size=shape) < 0.2, rng.uniform(-1e-4, 1e-4, shape), 0.0)
+    C = rng.uniform(0, 1, shape)
+    D = 1e-6 * rng.uniform(0.5, 1.5, shape)
+    BC = (rng.uniform(size=shape) < 0.05).astype(float)
+    q = [rng.uniform(-1e-4, 1e-4, shape) for _ in range(3)]
+    out = {}
+    for variant in ((512, 4, 2), (256, 3, 2), (1024, 2, 2), (512, 2, 1), (256, 4, 1)):
+        m = model_for(cfg, cuda_device, "fp32dc")
+        m.sweep_variant = variant
+        nk = NumpyKernels(m)
+        rp = nk.compute_P(P.copy(), *pargs, z, z, z, 3600.0, BP, WP, SOR=1.7, max_it=20000,
+                          inc_it=1.25, max_dt=1e5, min_dt=1e-8, P_conv=1e-10)
+        ran = m.last_variant
+        rc = nk.compute_C(C.copy(), D, D, D, pargs[3], pargs[2], *q, 3600.0, BC, z, numpy.ones(shape),
+                          z, omega=1, SOR=1.1, max_it=100, inc_it=1.05, max_dt=1e5, min_dt=1e-8,
+                          C_conv=1e-10)
+        assert ran == variant, (ran, variant)
+        out[variant] = (rp, rc)
+    ref_p, ref_c = out[(512, 4, 2)]
+    assert ref_p[5] > 50
+    for v, (p, c) in out.items():
+        assert (p[0], p[1], p[4], p[5]) == (ref_p[0], ref_p[1], ref_p[4], ref_p[5]), v
+        assert numpy.array_equal(p[2], ref_p[2]), v
+        assert (c[0], c[1], c[3], c[4]) == (ref_c[0], ref_c[1], ref_c[3], ref_c[4]), v
+        assert numpy.array_equal(c[2], ref_c[2]), v

@@ -17,7 +17,9 @@ compile-time choice among 18 instances:
 restored afterwards) and sets the fastest as the model's ``sweep_variant``;
 the choice is kept per grid shape, so later models of the same shape take it
 without timing.  The variant changes only how the same cell updates are
-scheduled: results are identical bit for bit.  SOR's omega is not a knob
+scheduled: every cell update is the same; only the grouping of the
+convergence check's sums follows the chunking, so the solves agree bit for bit
+unless a norm falls within rounding of its tolerance.  SOR's omega is not a knob
 here: it is the config's, and it sets the reference's iteration sequence.
 """
 from __future__ import annotations
