@@ -620,7 +620,7 @@ template <class Form>
 static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, double min_dt,
                   double conv, int max_it, int pressure_schedule, int stop_on_first,
                   TseDcOptions* opts, double sor, int x_index, double* X_out,
-                  TseSolveStatus* d_status, cudaStream_t stream) {
+                  TseSolveStatus* d_status, cudaStream_t stream, int first_parts = 0) {
     const int cycle = opts ? opts->cycle : 0;
     const int cap = opts ? opts->max_blocks : 0;
     if (S.tail_bytes < dc_extra_bytes(S.L)) return TSE_ERR_WORKSPACE;
@@ -669,8 +669,12 @@ static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, 
         opts->ring = nb_tma > 0 ? T.stages / pipes : 0;
     }
     const int nb = nb_tma > 0 ? nb_tma : sweep_blocks(S.L.Nc, cap);
-    dc_scale_kernel<<<gcells, kBlock, 0, stream>>>(S.F, c);
-    if (cudaGetLastError() != cudaSuccess) return TSE_ERR_LAUNCH;
+    // first_parts > 0: the setup has written the records, r' and that many
+    // x^2 partials (the first cycle's scale and residual)
+    if (first_parts == 0) {
+        dc_scale_kernel<<<gcells, kBlock, 0, stream>>>(S.F, c);
+        if (cudaGetLastError() != cudaSuccess) return TSE_ERR_LAUNCH;
+    }
     const bool timing = opts && opts->timing;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     if (timing) {
@@ -684,9 +688,14 @@ static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, 
     int prev_it = 0;
     int rc = TSE_OK;
     for (;;) {
-        const unsigned rb = (unsigned)res_blocks(S.L.Nc);
-        dc_residual_kernel<<<rb, kBlock, 0, stream>>>(S.F, c);
-        dc_x2_kernel<<<1, kBlock, 0, stream>>>(c, (int)rb);
+        if (first_parts > 0) {
+            dc_x2_kernel<<<1, kBlock, 0, stream>>>(c, first_parts);
+            first_parts = 0;
+        } else {
+            const unsigned rb = (unsigned)res_blocks(S.L.Nc);
+            dc_residual_kernel<<<rb, kBlock, 0, stream>>>(S.F, c);
+            dc_x2_kernel<<<1, kBlock, 0, stream>>>(c, (int)rb);
+        }
         void* args[] = {(void*)&c};
         void* targs[] = {(void*)&c, (void*)&T};
         // staged sweep: its barrier counter starts at 0
@@ -832,10 +841,11 @@ extern "C" int32_t tse_compute_C_dc(const TseGrid* grid, const TseSpeciesArgs* a
         return TSE_ERR_ARG;
     cudaStream_t stream = (cudaStream_t)stream_;
     TransportSetup S;
-    int rc = setup_species(grid, a, d_ws, ws_bytes, stream, S);
+    int nparts = 0;
+    int rc = setup_species_dc(grid, a, d_ws, ws_bytes, stream, S, &nparts);
     if (rc != TSE_OK) return rc;
     return run_dc(S, a->dt, a->inc_it, a->max_dt, a->min_dt, a->conv, a->max_it, 0,
-                  a->omega == 0.0, opts, a->SOR, TA_X, a->C, d_status, stream);
+                  a->omega == 0.0, opts, a->SOR, TA_X, a->C, d_status, stream, nparts);
 }
 
 extern "C" int32_t tse_compute_T_dc(const TseGrid* grid, const TseHeatArgs* a,
@@ -849,8 +859,9 @@ extern "C" int32_t tse_compute_T_dc(const TseGrid* grid, const TseHeatArgs* a,
         return TSE_ERR_ARG;
     cudaStream_t stream = (cudaStream_t)stream_;
     TransportSetup S;
-    int rc = setup_heat(grid, a, d_ws, ws_bytes, stream, S);
+    int nparts = 0;
+    int rc = setup_heat_dc(grid, a, d_ws, ws_bytes, stream, S, &nparts);
     if (rc != TSE_OK) return rc;
     return run_dc(S, a->dt, a->inc_it, a->max_dt, a->min_dt, a->conv, a->max_it, 0,
-                  a->omega == 0.0, opts, a->SOR, TA_X, a->T, d_status, stream);
+                  a->omega == 0.0, opts, a->SOR, TA_X, a->T, d_status, stream, nparts);
 }

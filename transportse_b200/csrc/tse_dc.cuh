@@ -165,6 +165,15 @@ int dc_halve(const Form& F, const DcCtl& c, cudaStream_t stream);
 int dc_apply(const DcCtl& c, cudaStream_t stream);
 int dc_finish(const DcCtl& c, TseSolveStatus* d_status, double* X_out, cudaStream_t stream);
 
+// Transport setups for the mixed-precision form (tse_transport.cu): the
+// exact form's arrays plus, from the same pass, the FP32 records, r' of the
+// initial iterate and *nparts per-block x^2 partials (S.partials) -- the
+// first correction cycle's scale and residual.
+int setup_species_dc(const TseGrid* grid, const TseSpeciesArgs* a, void* d_ws, size_t ws_bytes,
+                     cudaStream_t stream, TransportSetup& S, int* nparts);
+int setup_heat_dc(const TseGrid* grid, const TseHeatArgs* a, void* d_ws, size_t ws_bytes,
+                  cudaStream_t stream, TransportSetup& S, int* nparts);
+
 // Fill a control record for a solve whose exact-form setup is S (the FP32
 // arrays live in S.tail); returns the first byte after the FP32 arrays.
 template <class Form>

@@ -9,6 +9,7 @@
 //   X = (1-SOR) X + SOR (omega (Mnew+Nnew+Onew+Pnew+Qnew+Rnew)
 //                        + (1-omega) (...) + R Xn + W - E) / (R - omega M)
 // (tse.py:870-875, 1038-1043) term by term.  Compiled with --fmad=false.
+#include "tse_dc.cuh"
 #include "tse_forms.cuh"
 #include "tse_rbsolve.cuh"
 #include "tse_rbsolve_tma.cuh"
@@ -25,60 +26,62 @@ __device__ void dispersivity_dev(const double* qx, const double* qy, const doubl
     double qxl = 0, qyl = 0, qzl = 0, qxr = 0, qyr = 0, qzr = 0;
     double qxyl = 0, qxzl = 0, qyxl = 0, qyzl = 0, qzxl = 0, qzyl = 0;
     double qxyr = 0, qxzr = 0, qyxr = 0, qyzr = 0, qzxr = 0, qzyr = 0;
+    // cnt: 1/2 or 1/4 -- dividing by 2 or 4 and multiplying by 0.5 or 0.25
+    // round the same exact quotient, so the results are identical
     double q1, q2, q3, q4, cnt;
     if (i != 0) {
         qxl = qx[IX3(i - 1, j, k)];
-        q1 = qy[IX3(i - 1, j, k)]; q2 = qy[c]; q3 = q4 = 0; cnt = 2;
-        if (j != 0) { q3 = qy[IX3(i, j - 1, k)]; q4 = qy[IX3(i - 1, j - 1, k)]; cnt += 2; }
-        if (!(B[IX3(i - 1, j, k)] != 0)) qxyl = (q1 + q2 + q3 + q4) / cnt;
-        q1 = qz[IX3(i - 1, j, k)]; q2 = qz[c]; q3 = q4 = 0; cnt = 2;
-        if (k != 0) { q3 = qz[IX3(i, j, k - 1)]; q4 = qz[IX3(i - 1, j, k - 1)]; cnt += 2; }
-        if (!(B[IX3(i - 1, j, k)] != 0)) qxzl = (q1 + q2 + q3 + q4) / cnt;
+        q1 = qy[IX3(i - 1, j, k)]; q2 = qy[c]; q3 = q4 = 0; cnt = 0.5;
+        if (j != 0) { q3 = qy[IX3(i, j - 1, k)]; q4 = qy[IX3(i - 1, j - 1, k)]; cnt = 0.25; }
+        if (!(B[IX3(i - 1, j, k)] != 0)) qxyl = (q1 + q2 + q3 + q4) * cnt;
+        q1 = qz[IX3(i - 1, j, k)]; q2 = qz[c]; q3 = q4 = 0; cnt = 0.5;
+        if (k != 0) { q3 = qz[IX3(i, j, k - 1)]; q4 = qz[IX3(i - 1, j, k - 1)]; cnt = 0.25; }
+        if (!(B[IX3(i - 1, j, k)] != 0)) qxzl = (q1 + q2 + q3 + q4) * cnt;
     }
     if (i != nx - 1) {
         qxr = qx[c];
-        q1 = qy[c]; q2 = qy[IX3(i + 1, j, k)]; q3 = q4 = 0; cnt = 2;
-        if (j != 0) { q3 = qy[IX3(i + 1, j - 1, k)]; q4 = qy[IX3(i, j - 1, k)]; cnt += 2; }
-        if (!(B[IX3(i + 1, j, k)] != 0)) qxyr = (q1 + q2 + q3 + q4) / cnt;
-        q1 = qz[c]; q2 = qz[IX3(i + 1, j, k)]; q3 = q4 = 0; cnt = 2;
-        if (k != 0) { q3 = qz[IX3(i + 1, j, k - 1)]; q4 = qz[IX3(i, j, k - 1)]; cnt += 2; }
-        if (!(B[IX3(i + 1, j, k)] != 0)) qxzr = (q1 + q2 + q3 + q4) / cnt;
+        q1 = qy[c]; q2 = qy[IX3(i + 1, j, k)]; q3 = q4 = 0; cnt = 0.5;
+        if (j != 0) { q3 = qy[IX3(i + 1, j - 1, k)]; q4 = qy[IX3(i, j - 1, k)]; cnt = 0.25; }
+        if (!(B[IX3(i + 1, j, k)] != 0)) qxyr = (q1 + q2 + q3 + q4) * cnt;
+        q1 = qz[c]; q2 = qz[IX3(i + 1, j, k)]; q3 = q4 = 0; cnt = 0.5;
+        if (k != 0) { q3 = qz[IX3(i + 1, j, k - 1)]; q4 = qz[IX3(i, j, k - 1)]; cnt = 0.25; }
+        if (!(B[IX3(i + 1, j, k)] != 0)) qxzr = (q1 + q2 + q3 + q4) * cnt;
     }
     if (j != 0) {
         qyl = qy[IX3(i, j - 1, k)];
-        q1 = qx[c]; q2 = qx[IX3(i, j - 1, k)]; q3 = q4 = 0; cnt = 2;
-        if (i != 0) { q3 = qx[IX3(i - 1, j - 1, k)]; q4 = qx[IX3(i - 1, j, k)]; cnt += 2; }
-        if (!(B[IX3(i, j - 1, k)] != 0)) qyxl = (q1 + q2 + q3 + q4) / cnt;
-        q1 = qz[IX3(i, j - 1, k)]; q2 = qz[c]; q3 = q4 = 0; cnt = 2;
-        if (k != 0) { q3 = qz[IX3(i, j, k - 1)]; q4 = qz[IX3(i, j - 1, k - 1)]; cnt += 2; }
-        if (!(B[IX3(i, j - 1, k)] != 0)) qyzl = (q1 + q2 + q3 + q4) / cnt;
+        q1 = qx[c]; q2 = qx[IX3(i, j - 1, k)]; q3 = q4 = 0; cnt = 0.5;
+        if (i != 0) { q3 = qx[IX3(i - 1, j - 1, k)]; q4 = qx[IX3(i - 1, j, k)]; cnt = 0.25; }
+        if (!(B[IX3(i, j - 1, k)] != 0)) qyxl = (q1 + q2 + q3 + q4) * cnt;
+        q1 = qz[IX3(i, j - 1, k)]; q2 = qz[c]; q3 = q4 = 0; cnt = 0.5;
+        if (k != 0) { q3 = qz[IX3(i, j, k - 1)]; q4 = qz[IX3(i, j - 1, k - 1)]; cnt = 0.25; }
+        if (!(B[IX3(i, j - 1, k)] != 0)) qyzl = (q1 + q2 + q3 + q4) * cnt;
     }
     if (j != ny - 1) {
         qyr = qy[c];
-        q1 = qx[IX3(i, j + 1, k)]; q2 = qx[c]; q3 = q4 = 0; cnt = 2;
-        if (i != 0) { q3 = qx[IX3(i - 1, j, k)]; q4 = qx[IX3(i - 1, j + 1, k)]; cnt += 2; }
-        if (!(B[IX3(i, j + 1, k)] != 0)) qyxr = (q1 + q2 + q3 + q4) / cnt;
-        q1 = qz[c]; q2 = qz[IX3(i, j + 1, k)]; q3 = q4 = 0; cnt = 2;
-        if (k != 0) { q3 = qz[IX3(i, j + 1, k - 1)]; q4 = qz[IX3(i, j, k - 1)]; cnt += 2; }
-        if (!(B[IX3(i, j + 1, k)] != 0)) qyzr = (q1 + q2 + q3 + q4) / cnt;
+        q1 = qx[IX3(i, j + 1, k)]; q2 = qx[c]; q3 = q4 = 0; cnt = 0.5;
+        if (i != 0) { q3 = qx[IX3(i - 1, j, k)]; q4 = qx[IX3(i - 1, j + 1, k)]; cnt = 0.25; }
+        if (!(B[IX3(i, j + 1, k)] != 0)) qyxr = (q1 + q2 + q3 + q4) * cnt;
+        q1 = qz[c]; q2 = qz[IX3(i, j + 1, k)]; q3 = q4 = 0; cnt = 0.5;
+        if (k != 0) { q3 = qz[IX3(i, j + 1, k - 1)]; q4 = qz[IX3(i, j, k - 1)]; cnt = 0.25; }
+        if (!(B[IX3(i, j + 1, k)] != 0)) qyzr = (q1 + q2 + q3 + q4) * cnt;
     }
     if (k != 0) {
         qzl = qz[IX3(i, j, k - 1)];
-        q1 = qx[c]; q2 = qx[IX3(i, j, k - 1)]; q3 = q4 = 0; cnt = 2;
-        if (i != 0) { q3 = qx[IX3(i - 1, j, k - 1)]; q4 = qx[IX3(i - 1, j, k)]; cnt += 2; }
-        if (!(B[IX3(i, j, k - 1)] != 0)) qzxl = (q1 + q2 + q3 + q4) / cnt;
-        q1 = qy[c]; q2 = qy[IX3(i, j, k - 1)]; q3 = q4 = 0; cnt = 2;
-        if (j != 0) { q3 = qy[IX3(i, j - 1, k - 1)]; q4 = qy[IX3(i, j - 1, k)]; cnt += 2; }
-        if (!(B[IX3(i, j, k - 1)] != 0)) qzyl = (q1 + q2 + q3 + q4) / cnt;
+        q1 = qx[c]; q2 = qx[IX3(i, j, k - 1)]; q3 = q4 = 0; cnt = 0.5;
+        if (i != 0) { q3 = qx[IX3(i - 1, j, k - 1)]; q4 = qx[IX3(i - 1, j, k)]; cnt = 0.25; }
+        if (!(B[IX3(i, j, k - 1)] != 0)) qzxl = (q1 + q2 + q3 + q4) * cnt;
+        q1 = qy[c]; q2 = qy[IX3(i, j, k - 1)]; q3 = q4 = 0; cnt = 0.5;
+        if (j != 0) { q3 = qy[IX3(i, j - 1, k - 1)]; q4 = qy[IX3(i, j - 1, k)]; cnt = 0.25; }
+        if (!(B[IX3(i, j, k - 1)] != 0)) qzyl = (q1 + q2 + q3 + q4) * cnt;
     }
     if (k != nz - 1) {
         qzr = qz[c];
-        q1 = qx[IX3(i, j, k + 1)]; q2 = qx[c]; q3 = q4 = 0; cnt = 2;
-        if (i != 0) { q3 = qx[IX3(i - 1, j, k)]; q4 = qx[IX3(i - 1, j, k + 1)]; cnt += 2; }
-        if (!(B[IX3(i, j, k + 1)] != 0)) qzxr = (q1 + q2 + q3 + q4) / cnt;
-        q1 = qy[IX3(i, j, k + 1)]; q2 = qy[c]; q3 = q4 = 0; cnt = 2;
-        if (j != 0) { q3 = qy[IX3(i, j - 1, k)]; q4 = qy[IX3(i, j - 1, k + 1)]; cnt += 2; }
-        if (!(B[IX3(i, j, k + 1)] != 0)) qzyr = (q1 + q2 + q3 + q4) / cnt;
+        q1 = qx[IX3(i, j, k + 1)]; q2 = qx[c]; q3 = q4 = 0; cnt = 0.5;
+        if (i != 0) { q3 = qx[IX3(i - 1, j, k)]; q4 = qx[IX3(i - 1, j, k + 1)]; cnt = 0.25; }
+        if (!(B[IX3(i, j, k + 1)] != 0)) qzxr = (q1 + q2 + q3 + q4) * cnt;
+        q1 = qy[IX3(i, j, k + 1)]; q2 = qy[c]; q3 = q4 = 0; cnt = 0.5;
+        if (j != 0) { q3 = qy[IX3(i, j - 1, k)]; q4 = qy[IX3(i, j - 1, k + 1)]; cnt = 0.25; }
+        if (!(B[IX3(i, j, k + 1)] != 0)) qzyr = (q1 + q2 + q3 + q4) * cnt;
     }
 #undef IX3
     const double ll = l_l[c], lt = l_t[c];
@@ -108,26 +111,213 @@ __device__ __forceinline__ bool decode_padded(long long t, const Layout& L, Cell
     return true;
 }
 
-// Shared tail of both assemblies: store the per-cell terms.
-__device__ __forceinline__ void store_transport(const TransportForm& F, uint8_t* msk, const CellIdx& x,
-                                                const double* co, double Mo, double Xn,
-                                                double Rnum, double R, double M, double W,
-                                                double EX, double omega, bool active, int nx,
-                                                int ny, int nz) {
+// The assemblies below keep the reference's operations and their order for
+// every value they produce, and drop only divisions whose quotient is
+// already known:
+//  - harm2(H1, H2, d1, d2) = (d1 + d2) / (d1 / H1 + d2 / H2): a cell's own
+//    quotient d / H is the same in both faces of an axis, so it is formed once;
+//  - min0(q) / d and max0(q) / d: one of the two is 0 / d, so q / d is formed
+//    once and 0 / d (+0 for d > 0) is selected for the other.
+__device__ __forceinline__ double harm2w(double H1, double H2, double d1, double d2, double w1,
+                                         double w2) {
+    if (H1 != 0.0 && H2 != 0.0) return (d1 + d2) / (w1 + w2);
+    return 0.0;
+}
+__device__ __forceinline__ double zero_over(double d) { return d > 0.0 ? 0.0 : 0.0 / d; }
+
+// One axis of a transport assembly: the + face (toward the next cell along
+// the axis) and the - face.  dP/dM: diffusive (and dispersive) coefficients,
+// minP/maxP: min0/max0 of the cell's own face flux (scaled), maxM/minM: the
+// same for the - neighbour's face flux, coP/coM: upwinded neighbour
+// coefficients, oldP/oldM: coP * Xn(+ neighbour), coM * Xn(- neighbour).
+struct AxisTerms {
+    double dP, dM, minP, maxP, maxM, minM, coP, coM, oldP, oldM;
+};
+
+// compute_C, one axis (tse.py:811-861): x -> (A, B, N, H, M, G), y -> (C, D,
+// P, J, O, I), z -> (E, F, R, L, Q, K)
+__device__ __forceinline__ AxisTerms species_axis(const double* __restrict__ Df,
+                                                  const double* __restrict__ phi,
+                                                  const double* __restrict__ Xn,
+                                                  const double* __restrict__ q,
+                                                  const double* __restrict__ d, long long c,
+                                                  long long st, int ii, bool hp, bool hm,
+                                                  double phic, double DdP, double DdM) {
+    AxisTerms r = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const long long op = hp ? c + st : c, om = hm ? c - st : c;
+    const double dd = d[ii], dp = d[hp ? ii + 1 : ii], dm = d[hm ? ii - 1 : ii];
+    const double Dc = Df[c], Dp = Df[op], Dm = Df[om];
+    const double pp = phi[op], pm = phi[om];
+    const double xp = Xn[op], xm = Xn[om];
+    const double qc = q[c], qm = q[om];
+    const double wc = dd / Dc;
+    const double z = zero_over(dd);
+    if (hp) {
+        const double dd2 = (0.5 * (dp + dd)) * dd;
+        const double ph = amean2(pp, phic, dp, dd);
+        r.dP = (harm2w(Dp, Dc, dp, dd, dp / Dp, wc) * ph + DdP) / dd2;
+        const double qd = qc / dd;
+        r.minP = (0.0 < qc) ? z : qd;
+        r.maxP = (0.0 > qc) ? z : qd;
+        r.coP = r.dP - r.minP;
+        r.oldP = r.coP * xp;
+    }
+    if (hm) {
+        const double dd2 = (0.5 * (dm + dd)) * dd;
+        const double ph = amean2(pm, phic, dm, dd);
+        r.dM = (harm2w(Dm, Dc, dm, dd, dm / Dm, wc) * ph + DdM) / dd2;
+        const double qd = qm / dd;
+        r.maxM = (0.0 > qm) ? z : qd;
+        r.minM = (0.0 < qm) ? z : qd;
+        r.coM = r.dM + r.maxM;
+        r.oldM = r.coM * xm;
+    }
+    return r;
+}
+
+// compute_T, one axis (tse.py:952-1027): the face means of porosity,
+// conductivities, heat capacity and density, then the coefficients
+__device__ __forceinline__ AxisTerms heat_axis(const TseHeatArgs& a, const double* __restrict__ Xn,
+                                               const double* __restrict__ q,
+                                               const double* __restrict__ d, long long c,
+                                               long long st, int ii, bool hp, bool hm,
+                                               double DdP, double DdM) {
+    AxisTerms r = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    const long long op = hp ? c + st : c, om = hm ? c - st : c;
+    const double dd = d[ii], dp = d[hp ? ii + 1 : ii], dm = d[hm ? ii - 1 : ii];
+    const double phic = a.phi[c], lfc = a.l_f[c], lrc = a.l_r[c], cpc = a.cp_f[c], rhc = a.rho_f[c];
+    const double wlf = dd / lfc, wlr = dd / lrc, wcp = dd / cpc, wrh = dd / rhc;
+    const double qc = q[c], qm = q[om];
+    if (hp) {
+        const double dd2 = (0.5 * (dp + dd)) * dd;
+        const double php = a.phi[op], lfp = a.l_f[op], lrp = a.l_r[op], cpp = a.cp_f[op],
+                     rhp = a.rho_f[op];
+        const double por = amean2(phic, php, dd, dp);
+        const double lf = harm2w(lfc, lfp, dd, dp, wlf, dp / lfp);
+        const double lr = harm2w(lrc, lrp, dd, dp, wlr, dp / lrp);
+        const double cpf = harm2w(cpc, cpp, dd, dp, wcp, dp / cpp);
+        const double rhocpf = harm2w(rhc, rhp, dd, dp, wrh, dp / rhp) * cpf;
+        r.dP = ((1 - por) * lr + por * lf + DdP * rhocpf) / dd2;
+        const double S = rhocpf / dd;
+        r.minP = min0(qc) * S;
+        r.maxP = max0(qc) * S;
+        r.coP = r.dP - r.minP;
+        r.oldP = r.coP * Xn[op];
+    }
+    if (hm) {
+        const double dd2 = (0.5 * (dm + dd)) * dd;
+        const double phm = a.phi[om], lfm = a.l_f[om], lrm = a.l_r[om], cpm = a.cp_f[om],
+                     rhm = a.rho_f[om];
+        const double por = amean2(phic, phm, dd, dm);
+        const double lf = harm2w(lfc, lfm, dd, dm, wlf, dm / lfm);
+        const double lr = harm2w(lrc, lrm, dd, dm, wlr, dm / lrm);
+        const double cpf = harm2w(cpc, cpm, dd, dm, wcp, dm / cpm);
+        const double rhocpf = harm2w(rhc, rhm, dd, dm, wrh, dm / rhm) * cpf;
+        r.dM = ((1 - por) * lr + por * lf + DdM * rhocpf) / dd2;
+        const double S = rhocpf / dd;
+        r.maxM = max0(qm) * S;
+        r.minM = min0(qm) * S;
+        r.coM = r.dM + r.maxM;
+        r.oldM = r.coM * Xn[om];
+    }
+    return r;
+}
+
+// The per-cell terms of a transport solve: the six neighbour coefficients
+// (x+, x-, y+, y-, z+, z-), M, (1-omega)-part Mo, R and its numerator, source,
+// IMBLFLO term and the neighbour sum of the initial iterate in sum()'s order.
+struct TransportTerms {
+    double co[6];
+    double s, Mo, Xn, Rnum, R, M, W, EX;
+    bool active;
+};
+
+__device__ __forceinline__ void combine_axes(const AxisTerms& X, const AxisTerms& Y,
+                                             const AxisTerms& Z, double Xn, TransportTerms& T) {
+    T.co[0] = X.coP;
+    T.co[1] = X.coM;
+    T.co[2] = Y.coP;
+    T.co[3] = Y.coM;
+    T.co[4] = Z.coP;
+    T.co[5] = Z.coM;
+    // M = -A - B - C - D - E - F + G - H + I - J + K - L (tse.py:863, 1029)
+    T.M = -X.dP - X.dM - Y.dP - Y.dM - Z.dP - Z.dM + X.minM - X.maxP + Y.minM - Y.maxP + Z.minM -
+          Z.maxP;
+    T.Xn = Xn;
+    T.Mo = Xn * T.M + X.oldP + X.oldM + Y.oldP + Y.oldM + Z.oldP + Z.oldM;
+    double s = X.oldP;
+    s = s + X.oldM;
+    s = s + Y.oldP;
+    s = s + Y.oldM;
+    s = s + Z.oldP;
+    s = s + Z.oldM;
+    T.s = s;
+}
+
+// coefficient part of compute_C.solve (tse.py:795-868)
+__device__ __forceinline__ void species_terms(const TseGrid& g, const TseSpeciesArgs& a,
+                                              const CellIdx& x, const Layout& L, TransportTerms& T) {
+    const int nx = L.nx, ny = L.ny, nz = L.nz, i = x.i, j = x.j, k = x.k;
+    const long long c = x.c;
+    double Dd[6] = {0, 0, 0, 0, 0, 0};
+    if (a.l_l[c] != 0 || a.l_t[c] != 0)
+        dispersivity_dev(a.qx, a.qy, a.qz, a.l_l, a.l_t, a.BC, i, j, k, nx, ny, nz, Dd);
+    const double phic = a.phi[c];
+    const AxisTerms X = species_axis(a.D_fx, a.phi, a.C, a.qx, g.dx, c, (long long)ny * nz, i,
+                                     i != nx - 1, i != 0, phic, Dd[3], Dd[0]);
+    const AxisTerms Y = species_axis(a.D_fy, a.phi, a.C, a.qy, g.dy, c, nz, j, j != ny - 1, j != 0,
+                                     phic, Dd[4], Dd[1]);
+    const AxisTerms Z = species_axis(a.D_fz, a.phi, a.C, a.qz, g.dz, c, 1, k, k != nz - 1, k != 0,
+                                     phic, Dd[5], Dd[2]);
+    const double Xn = a.C[c];
+    combine_axes(X, Y, Z, Xn, T);
+    T.Rnum = a.RC[c] * phic;
+    T.R = T.Rnum / a.dt;
+    T.EX = a.imblflo ? Xn / a.rho_f[c] * a.e[c] : 0.0;
+    T.W = a.WC[c];
+    T.active = !(a.BC[c] != 0.0);
+}
+
+// coefficient part of compute_T.solve (tse.py:930-1036)
+__device__ __forceinline__ void heat_terms(const TseGrid& g, const TseHeatArgs& a, const CellIdx& x,
+                                           const Layout& L, TransportTerms& T) {
+    const int nx = L.nx, ny = L.ny, nz = L.nz, i = x.i, j = x.j, k = x.k;
+    const long long c = x.c;
+    double Dd[6] = {0, 0, 0, 0, 0, 0};
+    if (a.l_l[c] != 0 || a.l_t[c] != 0)
+        dispersivity_dev(a.qx, a.qy, a.qz, a.l_l, a.l_t, a.BT, i, j, k, nx, ny, nz, Dd);
+    const AxisTerms X = heat_axis(a, a.T, a.qx, g.dx, c, (long long)ny * nz, i, i != nx - 1, i != 0,
+                                  Dd[3], Dd[0]);
+    const AxisTerms Y = heat_axis(a, a.T, a.qy, g.dy, c, nz, j, j != ny - 1, j != 0, Dd[4], Dd[1]);
+    const AxisTerms Z = heat_axis(a, a.T, a.qz, g.dz, c, 1, k, k != nz - 1, k != 0, Dd[5], Dd[2]);
+    const double Xn = a.T[c];
+    combine_axes(X, Y, Z, Xn, T);
+    const double por_ = a.phi[c];
+    T.Rnum = por_ * a.rho_f[c] * a.cp_f[c] + (1 - por_) * a.rho_r[c] * a.cp_r[c];
+    T.R = T.Rnum / a.dt;
+    T.EX = a.imblflo ? a.cp_f[c] * Xn * a.e[c] : 0.0;
+    T.W = a.WT[c];
+    T.active = !(a.BT[c] != 0.0);
+}
+
+// The exact form's per-cell arrays (TransportForm) and the flag byte.
+__device__ __forceinline__ void store_terms(const TransportForm& F, uint8_t* msk, const CellIdx& x,
+                                            const TransportTerms& T, int nx, int ny, int nz) {
     double* b = F.arr[x.col];
     const long long N = F.Ncal, m = x.m;
-    for (int q = 0; q < 6; ++q) b[q * N + m] = co[q];
-    b[TA_Y * N + m] = (1 - omega) * Mo;
-    b[TA_RXN * N + m] = R * Xn;
-    b[TA_W * N + m] = W;
-    b[TA_EX * N + m] = EX;
-    b[TA_DEN * N + m] = R - omega * M;
-    b[TA_RNUM * N + m] = Rnum;
-    b[TA_M * N + m] = M;
-    b[TA_XN * N + m] = Xn;
-    b[TA_X * N + m] = Xn;
+    const double omega = F.omega;
+    for (int q = 0; q < 6; ++q) b[q * N + m] = T.co[q];
+    b[TA_Y * N + m] = (1 - omega) * T.Mo;
+    b[TA_RXN * N + m] = T.R * T.Xn;
+    b[TA_W * N + m] = T.W;
+    b[TA_EX * N + m] = T.EX;
+    b[TA_DEN * N + m] = T.R - omega * T.M;
+    b[TA_RNUM * N + m] = T.Rnum;
+    b[TA_M * N + m] = T.M;
+    b[TA_XN * N + m] = T.Xn;
+    b[TA_X * N + m] = T.Xn;
     uint8_t f = neighbour_flags(x.i, x.j, x.k, nx, ny, nz);
-    if (active) f |= F_ACTIVE;
+    if (T.active) f |= F_ACTIVE;
     msk[m] = f;
 }
 
@@ -137,214 +327,116 @@ __device__ __forceinline__ void store_padding(const TransportForm& F, uint8_t* m
     msk[x.m] = 0;
 }
 
-// Both assemblies run one thread per cell and are latency-bound (many FP64
-// divisions and neighbour loads per cell).  Three 256-thread blocks per SM
-// (80 registers, a few bytes spilled) rather than the two that 96-98
-// registers allow: measured on the 256 x 256 x 128 reservoir, species solves
-// 13.6 -> 16.2 and heat solves 9.1 -> 11.5 G cell-updates/s.
-constexpr int kAssembleMinBlocks = 3;
+// The mixed-precision form's first correction cycle, written by the same
+// pass: per colour the FP32 record K'_q = omega co_q / Den and
+// r' = (sum(Xn) - Den Xn) / Den of the initial iterate (sum() in
+// TransportForm's order; the neighbour products are the assembly's own
+// co_q * Xn_q), and per block the sum of Xn^2.  No bit-exactness is claimed
+// for this form: 1/Den is formed once.
+struct DcFuse {
+    float* K[2];
+    long long Ncal;
+    double* partials;
+    int per_thread;   // cells a thread assembles (blocks of kBlock consecutive cells)
+};
+
+__device__ __forceinline__ void store_dc(const TransportForm& F, const DcFuse& fz, const CellIdx& x,
+                                         const TransportTerms* T) {
+    float* Kc = fz.K[x.col];
+    float2* rec = reinterpret_cast<float2*>(Kc + 6 * x.m);
+    float rp = 0.0f;
+    if (T && T->active) {
+        const double omega = F.omega;
+        const double den = T->R - omega * T->M;
+        const double rden = 1.0 / den;
+#pragma unroll
+        for (int q = 0; q < 3; ++q)
+            rec[q] = make_float2((float)(omega * T->co[2 * q] * rden),
+                                 (float)(omega * T->co[2 * q + 1] * rden));
+        double num = omega * T->s;
+        if (F.useY) num = num + (1 - omega) * T->Mo;
+        num = num + T->R * T->Xn;
+        num = num + T->W;
+        num = num - (F.useEX ? T->EX : 0.0);
+        rp = (float)((num - den * T->Xn) * rden);
+    } else {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) rec[q] = make_float2(0.0f, 0.0f);
+    }
+    Kc[6 * fz.Ncal + x.m] = rp;
+}
+
+struct SpeciesKind {
+    using Args = TseSpeciesArgs;
+    static __device__ __forceinline__ void terms(const TseGrid& g, const Args& a, const CellIdx& x,
+                                                 const Layout& L, TransportTerms& T) {
+        species_terms(g, a, x, L, T);
+    }
+};
+struct HeatKind {
+    using Args = TseHeatArgs;
+    static __device__ __forceinline__ void terms(const TseGrid& g, const Args& a, const CellIdx& x,
+                                                 const Layout& L, TransportTerms& T) {
+        heat_terms(g, a, x, L, T);
+    }
+};
+
+// Both assemblies are latency-bound (FP64 divisions and neighbour loads per
+// cell).  Three 256-thread blocks per SM (80 registers) rather than the two
+// that ~96 registers allow: measured on the 256 x 256 x 128 reservoir,
+// species solves 13.6 -> 16.2 and heat solves 9.1 -> 11.5 G cell-updates/s.
+#ifndef TSE_ASM_MINB
+#define TSE_ASM_MINB 3
+#endif
+constexpr int kAssembleMinBlocks = TSE_ASM_MINB;
+
+// One thread per cell of the padded natural order (DC: per_thread
+// consecutive blocks of kBlock cells each, so the x^2 partials stay few).
+template <class Kind, bool DC>
+__device__ __forceinline__ void assemble_body(const TseGrid& g, const typename Kind::Args& a,
+                                              const TransportForm& F, uint8_t* mask0,
+                                              uint8_t* mask1, const Layout& L, const DcFuse& fz) {
+    __shared__ double sh[kBlock / 32];
+    double x2 = 0.0;
+    const int per = DC ? fz.per_thread : 1;
+    for (int s = 0; s < per; ++s) {
+        CellIdx x;
+        const long long t = ((long long)blockIdx.x * per + s) * kBlock + threadIdx.x;
+        if (!decode_padded(t, L, x)) break;
+        uint8_t* msk = x.col ? mask1 : mask0;
+        if (x.pad) {
+            store_padding(F, msk, x);
+            if (DC) store_dc(F, fz, x, nullptr);
+            continue;
+        }
+        TransportTerms T;
+        Kind::terms(g, a, x, L, T);
+        store_terms(F, msk, x, T, L.nx, L.ny, L.nz);
+        if (DC) {
+            store_dc(F, fz, x, &T);
+            x2 = x2 + T.Xn * T.Xn;
+        }
+    }
+    if (DC) {
+        const double b = block_sum<kBlock>(x2, sh);
+        if (threadIdx.x == 0) fz.partials[blockIdx.x] = b;
+    }
+}
 
 // coefficient part of compute_C.solve (tse.py:795-868)
-__global__ void __launch_bounds__(kBlock, kAssembleMinBlocks) assemble_c_kernel(TseGrid g, TseSpeciesArgs a, TransportForm F, uint8_t* mask0,
-                                  uint8_t* mask1, Layout L) {
-    CellIdx x;
-    if (!decode_padded((long long)blockIdx.x * blockDim.x + threadIdx.x, L, x)) return;
-    uint8_t* msk = x.col ? mask1 : mask0;
-    if (x.pad) { store_padding(F, msk, x); return; }
-    const int nx = L.nx, ny = L.ny, nz = L.nz, i = x.i, j = x.j, k = x.k;
-    const long long c = x.c, sx = (long long)ny * nz;
-    const double *dx = g.dx, *dy = g.dy, *dz = g.dz, *phi = a.phi, *Cn = a.C;
-    double A_ = 0, B_ = 0, C_ = 0, D_ = 0, E_ = 0, F_ = 0, G_ = 0, H_ = 0, I_ = 0, J_ = 0, K_ = 0,
-           L_ = 0, M_ = 0, N_ = 0, O_ = 0, P_ = 0, Q_ = 0, R_ = 0, EC = 0;
-    double Mold = 0, Nold = 0, Oold = 0, Pold = 0, Qold = 0, Rold = 0;
-    double Dd[6] = {0, 0, 0, 0, 0, 0};
-    double dd, dd2, ph;
-    if (a.l_l[c] != 0 || a.l_t[c] != 0)
-        dispersivity_dev(a.qx, a.qy, a.qz, a.l_l, a.l_t, a.BC, i, j, k, nx, ny, nz, Dd);
-    double co[6] = {0, 0, 0, 0, 0, 0};
-    if (i != nx - 1) {
-        const long long o = c + sx;
-        dd = dx[i];
-        dd2 = (0.5 * (dx[i + 1] + dx[i])) * dd;
-        ph = amean2(phi[o], phi[c], dx[i + 1], dx[i]);
-        A_ = (harm2(a.D_fx[o], a.D_fx[c], dx[i + 1], dx[i]) * ph + Dd[3]) / dd2;
-        N_ = min0(a.qx[c]) / dd;
-        H_ = max0(a.qx[c]) / dd;
-        co[0] = A_ - N_;
-        Mold = co[0] * Cn[o];
-    }
-    if (i != 0) {
-        const long long o = c - sx;
-        dd = dx[i];
-        dd2 = (0.5 * (dx[i - 1] + dx[i])) * dd;
-        ph = amean2(phi[o], phi[c], dx[i - 1], dx[i]);
-        B_ = (harm2(a.D_fx[o], a.D_fx[c], dx[i - 1], dx[i]) * ph + Dd[0]) / dd2;
-        M_ = max0(a.qx[o]) / dd;
-        G_ = min0(a.qx[o]) / dd;
-        co[1] = B_ + M_;
-        Nold = co[1] * Cn[o];
-    }
-    if (j != ny - 1) {
-        const long long o = c + nz;
-        dd = dy[j];
-        dd2 = (0.5 * (dy[j + 1] + dy[j])) * dd;
-        ph = amean2(phi[o], phi[c], dy[j + 1], dy[j]);
-        C_ = (harm2(a.D_fy[o], a.D_fy[c], dy[j + 1], dy[j]) * ph + Dd[4]) / dd2;
-        P_ = min0(a.qy[c]) / dd;
-        J_ = max0(a.qy[c]) / dd;
-        co[2] = C_ - P_;
-        Oold = co[2] * Cn[o];
-    }
-    if (j != 0) {
-        const long long o = c - nz;
-        dd = dy[j];
-        dd2 = (0.5 * (dy[j - 1] + dy[j])) * dd;
-        ph = amean2(phi[o], phi[c], dy[j - 1], dy[j]);
-        D_ = (harm2(a.D_fy[o], a.D_fy[c], dy[j - 1], dy[j]) * ph + Dd[1]) / dd2;
-        O_ = max0(a.qy[o]) / dd;
-        I_ = min0(a.qy[o]) / dd;
-        co[3] = D_ + O_;
-        Pold = co[3] * Cn[o];
-    }
-    if (k != nz - 1) {
-        const long long o = c + 1;
-        dd = dz[k];
-        dd2 = (0.5 * (dz[k + 1] + dz[k])) * dd;
-        ph = amean2(phi[o], phi[c], dz[k + 1], dz[k]);
-        E_ = (harm2(a.D_fz[o], a.D_fz[c], dz[k + 1], dz[k]) * ph + Dd[5]) / dd2;
-        R_ = min0(a.qz[c]) / dd;
-        L_ = max0(a.qz[c]) / dd;
-        co[4] = E_ - R_;
-        Qold = co[4] * Cn[o];
-    }
-    if (k != 0) {
-        const long long o = c - 1;
-        dd = dz[k];
-        dd2 = (0.5 * (dz[k - 1] + dz[k])) * dd;
-        ph = amean2(phi[o], phi[c], dz[k - 1], dz[k]);
-        F_ = (harm2(a.D_fz[o], a.D_fz[c], dz[k - 1], dz[k]) * ph + Dd[2]) / dd2;
-        Q_ = max0(a.qz[o]) / dd;
-        K_ = min0(a.qz[o]) / dd;
-        co[5] = F_ + Q_;
-        Rold = co[5] * Cn[o];
-    }
-    const double Rnum = a.RC[c] * phi[c];
-    const double R = Rnum / a.dt;
-    const double M = -A_ - B_ - C_ - D_ - E_ - F_ + G_ - H_ + I_ - J_ + K_ - L_;
-    if (a.imblflo) EC = Cn[c] / a.rho_f[c] * a.e[c];
-    const double Xn = Cn[c];
-    const double Mo = Xn * M + Mold + Nold + Oold + Pold + Qold + Rold;
-    store_transport(F, msk, x, co, Mo, Xn, Rnum, R, M, a.WC[c], EC, a.omega, !(a.BC[c] != 0.0),
-                    nx, ny, nz);
+template <bool DC>
+__global__ void __launch_bounds__(kBlock, kAssembleMinBlocks)
+    assemble_c_kernel(TseGrid g, TseSpeciesArgs a, TransportForm F, uint8_t* mask0, uint8_t* mask1,
+                      Layout L, DcFuse fz) {
+    assemble_body<SpeciesKind, DC>(g, a, F, mask0, mask1, L, fz);
 }
 
 // coefficient part of compute_T.solve (tse.py:930-1036)
-__global__ void __launch_bounds__(kBlock, kAssembleMinBlocks) assemble_t_kernel(TseGrid g, TseHeatArgs a, TransportForm F, uint8_t* mask0,
-                                  uint8_t* mask1, Layout L) {
-    CellIdx x;
-    if (!decode_padded((long long)blockIdx.x * blockDim.x + threadIdx.x, L, x)) return;
-    uint8_t* msk = x.col ? mask1 : mask0;
-    if (x.pad) { store_padding(F, msk, x); return; }
-    const int nx = L.nx, ny = L.ny, nz = L.nz, i = x.i, j = x.j, k = x.k;
-    const long long c = x.c, sx = (long long)ny * nz;
-    const double *dx = g.dx, *dy = g.dy, *dz = g.dz, *phi = a.phi, *Tn = a.T;
-    double A_ = 0, B_ = 0, C_ = 0, D_ = 0, E_ = 0, F_ = 0, G_ = 0, H_ = 0, I_ = 0, J_ = 0, K_ = 0,
-           L_ = 0, S_ = 0, M_ = 0, N_ = 0, O_ = 0, P_ = 0, Q_ = 0, R_ = 0, ET = 0;
-    double Mold = 0, Nold = 0, Oold = 0, Pold = 0, Qold = 0, Rold = 0;
-    double Dd[6] = {0, 0, 0, 0, 0, 0};
-    double dd, dd2, por, lf, lr, cpf, rhocpf;
-    if (a.l_l[c] != 0 || a.l_t[c] != 0)
-        dispersivity_dev(a.qx, a.qy, a.qz, a.l_l, a.l_t, a.BT, i, j, k, nx, ny, nz, Dd);
-    double co[6] = {0, 0, 0, 0, 0, 0};
-#define TFACE(o, d1, d2)                                   \
-    por = amean2(phi[c], phi[o], d1, d2);                  \
-    lf = harm2(a.l_f[c], a.l_f[o], d1, d2);                \
-    lr = harm2(a.l_r[c], a.l_r[o], d1, d2);                \
-    cpf = harm2(a.cp_f[c], a.cp_f[o], d1, d2);             \
-    rhocpf = harm2(a.rho_f[c], a.rho_f[o], d1, d2) * cpf;
-    if (i != nx - 1) {
-        const long long o = c + sx;
-        dd = dx[i];
-        dd2 = (0.5 * (dx[i + 1] + dx[i])) * dd;
-        TFACE(o, dx[i], dx[i + 1]);
-        A_ = ((1 - por) * lr + por * lf + Dd[3] * rhocpf) / dd2;
-        S_ = rhocpf / dd;
-        N_ = min0(a.qx[c]) * S_;
-        H_ = max0(a.qx[c]) * S_;
-        co[0] = A_ - N_;
-        Mold = co[0] * Tn[o];
-    }
-    if (i != 0) {
-        const long long o = c - sx;
-        dd = dx[i];
-        dd2 = (0.5 * (dx[i - 1] + dx[i])) * dd;
-        TFACE(o, dx[i], dx[i - 1]);
-        B_ = ((1 - por) * lr + por * lf + Dd[0] * rhocpf) / dd2;
-        S_ = rhocpf / dd;
-        M_ = max0(a.qx[o]) * S_;
-        G_ = min0(a.qx[o]) * S_;
-        co[1] = B_ + M_;
-        Nold = co[1] * Tn[o];
-    }
-    if (j != ny - 1) {
-        const long long o = c + nz;
-        dd = dy[j];
-        dd2 = (0.5 * (dy[j + 1] + dy[j])) * dd;
-        TFACE(o, dy[j], dy[j + 1]);
-        C_ = ((1 - por) * lr + por * lf + Dd[4] * rhocpf) / dd2;
-        S_ = rhocpf / dd;
-        P_ = min0(a.qy[c]) * S_;
-        J_ = max0(a.qy[c]) * S_;
-        co[2] = C_ - P_;
-        Oold = co[2] * Tn[o];
-    }
-    if (j != 0) {
-        const long long o = c - nz;
-        dd = dy[j];
-        dd2 = (0.5 * (dy[j - 1] + dy[j])) * dd;
-        TFACE(o, dy[j], dy[j - 1]);
-        D_ = ((1 - por) * lr + por * lf + Dd[1] * rhocpf) / dd2;
-        S_ = rhocpf / dd;
-        O_ = max0(a.qy[o]) * S_;
-        I_ = min0(a.qy[o]) * S_;
-        co[3] = D_ + O_;
-        Pold = co[3] * Tn[o];
-    }
-    if (k != nz - 1) {
-        const long long o = c + 1;
-        dd = dz[k];
-        dd2 = (0.5 * (dz[k + 1] + dz[k])) * dd;
-        TFACE(o, dz[k], dz[k + 1]);
-        E_ = ((1 - por) * lr + por * lf + Dd[5] * rhocpf) / dd2;
-        S_ = rhocpf / dd;
-        R_ = min0(a.qz[c]) * S_;
-        L_ = max0(a.qz[c]) * S_;
-        co[4] = E_ - R_;
-        Qold = co[4] * Tn[o];
-    }
-    if (k != 0) {
-        const long long o = c - 1;
-        dd = dz[k];
-        dd2 = (0.5 * (dz[k - 1] + dz[k])) * dd;
-        TFACE(o, dz[k], dz[k - 1]);
-        F_ = ((1 - por) * lr + por * lf + Dd[2] * rhocpf) / dd2;
-        S_ = rhocpf / dd;
-        Q_ = max0(a.qz[o]) * S_;
-        K_ = min0(a.qz[o]) * S_;
-        co[5] = F_ + Q_;
-        Rold = co[5] * Tn[o];
-    }
-#undef TFACE
-    (void)S_;
-    const double por_ = phi[c];
-    const double Rnum = por_ * a.rho_f[c] * a.cp_f[c] + (1 - por_) * a.rho_r[c] * a.cp_r[c];
-    const double R = Rnum / a.dt;
-    const double M = -A_ - B_ - C_ - D_ - E_ - F_ + G_ - H_ + I_ - J_ + K_ - L_;
-    if (a.imblflo) ET = a.cp_f[c] * Tn[c] * a.e[c];
-    const double Xn = Tn[c];
-    const double Mo = Xn * M + Mold + Nold + Oold + Pold + Qold + Rold;
-    store_transport(F, msk, x, co, Mo, Xn, Rnum, R, M, a.WT[c], ET, a.omega, !(a.BT[c] != 0.0),
-                    nx, ny, nz);
+template <bool DC>
+__global__ void __launch_bounds__(kBlock, kAssembleMinBlocks)
+    assemble_t_kernel(TseGrid g, TseHeatArgs a, TransportForm F, uint8_t* mask0, uint8_t* mask1,
+                      Layout L, DcFuse fz) {
+    assemble_body<HeatKind, DC>(g, a, F, mask0, mask1, L, fz);
 }
 
 __global__ void unpack_t_kernel(double* out, const double* X0, const double* X1, Layout L) {
@@ -371,9 +463,11 @@ size_t transport_ws_bytes(const Layout& L, long long* Ncal_out) {
 
 // Carve the workspace and launch the assembly (shared by the exact and the
 // defect-correction transport solves).
-template <class Args, class AssembleK>
-static int setup_transport(const TseGrid* grid, const Args* a, void* d_ws, size_t ws_bytes,
-                           cudaStream_t stream, AssembleK kernel, int imbl, TransportSetup& S) {
+// Carve the workspace (shared by the exact and the defect-correction
+// transport solves) and reset the grid barrier.
+template <class Args>
+static int carve_transport(const TseGrid* grid, const Args* a, void* d_ws, size_t ws_bytes,
+                           cudaStream_t stream, int imbl, TransportSetup& S) {
     S.L = make_layout(grid->nx, grid->ny, grid->nz);
     const size_t need = transport_ws_bytes(S.L, &S.Ncal);
     if (need > ws_bytes) return TSE_ERR_WORKSPACE;
@@ -398,20 +492,69 @@ static int setup_transport(const TseGrid* grid, const Args* a, void* d_ws, size_
     S.tail = (char*)d_ws + need;
     S.tail_bytes = ws_bytes - need;
     if (cudaMemsetAsync(S.bar, 0, sizeof(GridBarrier), stream) != cudaSuccess) return TSE_ERR_LAUNCH;
+    return TSE_OK;
+}
+
+// carve + the exact form's assembly
+template <class Args, class AssembleK>
+static int setup_transport(const TseGrid* grid, const Args* a, void* d_ws, size_t ws_bytes,
+                           cudaStream_t stream, AssembleK kernel, int imbl, TransportSetup& S) {
+    int rc = carve_transport(grid, a, d_ws, ws_bytes, stream, imbl, S);
+    if (rc != TSE_OK) return rc;
     const long long total = (long long)S.L.nx * S.L.ny * S.L.nzp;
-    kernel<<<(unsigned)((total + kBlock - 1) / kBlock), kBlock, 0, stream>>>(*grid, *a, S.F, S.mask[0],
-                                                                              S.mask[1], S.L);
+    kernel<<<(unsigned)((total + kBlock - 1) / kBlock), kBlock, 0, stream>>>(
+        *grid, *a, S.F, S.mask[0], S.mask[1], S.L, DcFuse{});
+    return cudaGetLastError() == cudaSuccess ? TSE_OK : TSE_ERR_LAUNCH;
+}
+
+// carve + the assembly that also writes the mixed-precision form's first
+// cycle (records, r', x^2 partials); *nparts: the number of partials.  The
+// block count is a function of the grid alone (at most kMaxBlocks), so the
+// x^2 sums are grouped the same way on every device.
+template <class Args, class AssembleK>
+static int setup_transport_dc(const TseGrid* grid, const Args* a, void* d_ws, size_t ws_bytes,
+                              cudaStream_t stream, AssembleK kernel, int imbl, TransportSetup& S,
+                              int* nparts) {
+    int rc = carve_transport(grid, a, d_ws, ws_bytes, stream, imbl, S);
+    if (rc != TSE_OK) return rc;
+    if (S.tail_bytes < dc_extra_bytes(S.L)) return TSE_ERR_WORKSPACE;
+    DcCtl c;
+    dc_carve(S, c, TA_X);
+    const long long total = (long long)S.L.nx * S.L.ny * S.L.nzp;
+    const long long groups = (total + kBlock - 1) / kBlock;
+    const long long per = (groups + kMaxBlocks - 1) / kMaxBlocks;
+    const long long nb = (groups + per - 1) / per;
+    DcFuse fz;
+    fz.K[0] = c.K[0];
+    fz.K[1] = c.K[1];
+    fz.Ncal = c.Ncal;
+    fz.partials = S.partials;
+    fz.per_thread = (int)per;
+    kernel<<<(unsigned)nb, kBlock, 0, stream>>>(*grid, *a, S.F, S.mask[0], S.mask[1], S.L, fz);
+    *nparts = (int)nb;
     return cudaGetLastError() == cudaSuccess ? TSE_OK : TSE_ERR_LAUNCH;
 }
 
 int setup_species(const TseGrid* grid, const TseSpeciesArgs* a, void* d_ws, size_t ws_bytes,
                   cudaStream_t stream, TransportSetup& S) {
-    return setup_transport(grid, a, d_ws, ws_bytes, stream, assemble_c_kernel, a->imblflo, S);
+    return setup_transport(grid, a, d_ws, ws_bytes, stream, assemble_c_kernel<false>, a->imblflo, S);
 }
 
 int setup_heat(const TseGrid* grid, const TseHeatArgs* a, void* d_ws, size_t ws_bytes,
                cudaStream_t stream, TransportSetup& S) {
-    return setup_transport(grid, a, d_ws, ws_bytes, stream, assemble_t_kernel, a->imblflo, S);
+    return setup_transport(grid, a, d_ws, ws_bytes, stream, assemble_t_kernel<false>, a->imblflo, S);
+}
+
+int setup_species_dc(const TseGrid* grid, const TseSpeciesArgs* a, void* d_ws, size_t ws_bytes,
+                     cudaStream_t stream, TransportSetup& S, int* nparts) {
+    return setup_transport_dc(grid, a, d_ws, ws_bytes, stream, assemble_c_kernel<true>, a->imblflo,
+                              S, nparts);
+}
+
+int setup_heat_dc(const TseGrid* grid, const TseHeatArgs* a, void* d_ws, size_t ws_bytes,
+                  cudaStream_t stream, TransportSetup& S, int* nparts) {
+    return setup_transport_dc(grid, a, d_ws, ws_bytes, stream, assemble_t_kernel<true>, a->imblflo,
+                              S, nparts);
 }
 
 template <class Args, class AssembleK>
@@ -511,8 +654,8 @@ extern "C" int32_t tse_compute_C(const TseGrid* grid, const TseSpeciesArgs* a,
     if (!a->C || !a->D_fx || !a->D_fy || !a->D_fz || !a->phi || !a->rho_f || !a->qx || !a->qy ||
         !a->qz || !a->BC || !a->WC || !a->RC || !a->e || !a->l_l || !a->l_t)
         return TSE_ERR_ARG;
-    return run_transport(grid, a, a->C, d_status, d_ws, ws_bytes, stream, assemble_c_kernel,
-                         a->imblflo);
+    return run_transport(grid, a, a->C, d_status, d_ws, ws_bytes, stream,
+                         assemble_c_kernel<false>, a->imblflo);
 }
 
 extern "C" int32_t tse_compute_T(const TseGrid* grid, const TseHeatArgs* a,
@@ -523,8 +666,8 @@ extern "C" int32_t tse_compute_T(const TseGrid* grid, const TseHeatArgs* a,
     if (!a->T || !a->l_f || !a->cp_f || !a->rho_f || !a->phi || !a->qx || !a->qy || !a->qz ||
         !a->BT || !a->WT || !a->e || !a->l_r || !a->rho_r || !a->cp_r || !a->l_l || !a->l_t)
         return TSE_ERR_ARG;
-    return run_transport(grid, a, a->T, d_status, d_ws, ws_bytes, stream, assemble_t_kernel,
-                         a->imblflo);
+    return run_transport(grid, a, a->T, d_status, d_ws, ws_bytes, stream,
+                         assemble_t_kernel<false>, a->imblflo);
 }
 
 extern "C" int32_t tse_smolarkiewicz(const TseGrid* grid, const double* C, const double* qx,
