@@ -71,6 +71,8 @@ def parse_args():
                     help="time one pressure solve of exactly --iters red+black iterations "
                          "(for isolated kernel timing and profiler captures)")
     ap.add_argument("--iters", type=int, default=200)
+    ap.add_argument("--variant", type=str, default=None,
+                    help="kernel-only: staged sweep chunk,ring,pipes (e.g. 1024,2,2)")
     ap.add_argument("--repeat", type=int, default=3)
     ap.add_argument("--workload", choices=("reservoir", "ensemble", "serving", "sloped"),
                     default="reservoir")
@@ -578,6 +580,8 @@ def kernel_only(a):
                      precision=a.kernel_only)
     M, S = sim.M, sim.S
     M.dc_min_conv = 0.0   # P_conv = 0 below: keep the requested form
+    if a.variant:
+        M.sweep_variant = tuple(int(x) for x in a.variant.split(","))
     P0 = S["P"].clone()
     peak, kind = measured_peak()
     M.timing = a.kernel_only == "fp32dc"
@@ -613,6 +617,7 @@ def kernel_only(a):
               "cell_updates_per_s": sweep[0][1] * active / (sms / 1e3),
               "frac_of_peak": sweep[0][1] * active / (sms / 1e3) * ALG_BYTES["fp32dc"] / 1e9 / peak}
     print(json.dumps({"kernel_only": a.kernel_only, "shape": list(shape), "iterations": its,
+                      "variant": M.last_variant,
                       "residual_cycles": int(st.cycles), "halvings": int(st.halvings),
                       "sweep_kernel": sw,
                       "ms_per_launch": ms, "cell_updates_per_s": rate,

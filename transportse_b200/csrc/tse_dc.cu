@@ -107,7 +107,16 @@ __global__ void __launch_bounds__(kBlock) dc_residual_kernel(Form F, DcCtl c) {
 __global__ void dc_x2_kernel(DcCtl c, int nparts) {
     __shared__ double sh[kBlock / 32];
     double s = 0.0;
-    for (int b = threadIdx.x; b < nparts; b += blockDim.x) s = s + c.partials[b];
+    int b = threadIdx.x;
+    // eight loads in flight, summed in the order of the plain loop
+    for (; b + 7 * kBlock < nparts; b += 8 * kBlock) {
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = c.partials[b + u * kBlock];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) s = s + v[u];
+    }
+    for (; b < nparts; b += kBlock) s = s + c.partials[b];
     s = block_sum<kBlock>(s, sh);
     if (threadIdx.x == 0) {
         c.st->x2 = s;
@@ -122,6 +131,22 @@ __global__ void dc_apply_kernel(DcCtl c) {
     const int col = t >= c.L.Nc;
     const long long m = t - col * c.L.Nc;
     if (c.mask[col][m] & F_ACTIVE) c.X[col][m] = c.X[col][m] + (double)c.D[col][m];
+}
+
+// x += d and the natural-layout result in one pass: the last cycle of a
+// solve (dc_apply_kernel then unpack_kernel, without storing x)
+__global__ void dc_apply_unpack_kernel(double* out, DcCtl c) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long total = (long long)c.L.nx * c.L.ny * c.L.nz;
+    if (t >= total) return;
+    int i, j, k;
+    long long row;
+    grid_coords(t, c.L.ny, c.L.nz, i, j, k, row);
+    const long long m = (row * c.L.nzp + k) >> 1;
+    const int col = (i + j + k) & 1;
+    double x = c.X[col][m];
+    if (c.mask[col][m] & F_ACTIVE) x = x + (double)c.D[col][m];
+    out[t] = x;
 }
 
 // ------------------------------------------------------------ FP32 sweeps
@@ -687,6 +712,7 @@ static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, 
     }
     int prev_it = 0;
     int rc = TSE_OK;
+    bool final_apply = false;
     for (;;) {
         if (first_parts > 0) {
             dc_x2_kernel<<<1, kBlock, 0, stream>>>(c, first_parts);
@@ -743,9 +769,12 @@ static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, 
             continue;
         }
         if (event == EV_ERROR) break;
+        if (event == EV_CONVERGED || event == EV_STOP) {
+            final_apply = true;   // x += d fused with the unpack below
+            break;
+        }
         dc_apply_kernel<<<gcells, kBlock, 0, stream>>>(c);
         if (cudaGetLastError() != cudaSuccess) { rc = TSE_ERR_LAUNCH; break; }
-        if (event == EV_CONVERGED || event == EV_STOP) break;
     }
     if (timing) {
         cudaEventDestroy(ev0);
@@ -754,6 +783,11 @@ static int run_dc(SolveSetup<Form>& S, double dt, double inc_it, double max_dt, 
     if (rc != TSE_OK) return rc;
     dc_status_kernel<<<1, 1, 0, stream>>>(c.st, d_status);
     if (cudaGetLastError() != cudaSuccess) return TSE_ERR_LAUNCH;
+    if (final_apply) {
+        const long long nat = (long long)S.L.nx * S.L.ny * S.L.nz;
+        dc_apply_unpack_kernel<<<(unsigned)((nat + kBlock - 1) / kBlock), kBlock, 0, stream>>>(X_out, c);
+        return cudaGetLastError() == cudaSuccess ? TSE_OK : TSE_ERR_LAUNCH;
+    }
     return launch_unpack(X_out, c.X[0], c.X[1], S.L, stream);
 }
 

@@ -307,10 +307,12 @@ __device__ __forceinline__ void store_terms(const TransportForm& F, uint8_t* msk
     const long long N = F.Ncal, m = x.m;
     const double omega = F.omega;
     for (int q = 0; q < 6; ++q) b[q * N + m] = T.co[q];
-    b[TA_Y * N + m] = (1 - omega) * T.Mo;
+    // the (1-omega) part and the IMBLFLO term are read only where the form
+    // uses them (TransportForm::useY / useEX)
+    if (F.useY) b[TA_Y * N + m] = (1 - omega) * T.Mo;
     b[TA_RXN * N + m] = T.R * T.Xn;
     b[TA_W * N + m] = T.W;
-    b[TA_EX * N + m] = T.EX;
+    if (F.useEX) b[TA_EX * N + m] = T.EX;
     b[TA_DEN * N + m] = T.R - omega * T.M;
     b[TA_RNUM * N + m] = T.Rnum;
     b[TA_M * N + m] = T.M;
