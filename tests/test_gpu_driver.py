@@ -69,3 +69,28 @@ def test_driver_matches_reference_course_models(name, cuda_device, tmp_path):
             assert rel_err(got[k], fx[k]) <= TOL, (k, rel_err(got[k], fx[k]))
             if k.startswith("P@"):
                 assert dynamic_pressure_err(got[k], fx[k], P0) <= TOL, k
+
+
+def test_swap_state_continues_the_run(cuda_device):
+    """A run whose state moves into another set of buffers between steps
+    (Simulation.swap_state, as a caller streaming host inputs does) gives the
+    same fields bit for bit as the run that never swaps."""
+    import torch
+    from transportse_b200 import workloads
+    from transportse_b200.driver import Simulation
+    make = lambda: workloads.reservoir_3d(12, 10, 8, seed=3)   # noqa: E731
+    ref = Simulation(make(), device=cuda_device, precision="fp64")
+    ref.run(max_steps=3)
+    sim = Simulation(make(), device=cuda_device, precision="fp64")
+    sim.run(max_steps=1)
+    for _ in range(2):
+        other = {n: t.clone() for n, t in sim.S.items()}
+        old = sim.swap_state(other)
+        assert sim.S is other and old is not other
+        sim.run(max_steps=1)
+    for f in ("P", "C", "T", "qx", "qy", "qz", "rho_f"):
+        assert numpy.array_equal(sim.field(f), ref.field(f)), f
+    bad = {n: t.clone() for n, t in sim.S.items()}
+    bad["P"] = torch.zeros(3, device=sim.S["P"].device, dtype=torch.float64)
+    with pytest.raises(ValueError):
+        sim.swap_state(bad)

@@ -75,11 +75,18 @@ def tune_sweep(sim, iters=64, repeats=3, variants=VARIANTS, cache=True):
     P0 = sim.S["P"].clone()
     trials = []
     seen = set()
+    failed = []
     for v in variants:
         ms_list, ran = [], None
-        for _ in range(repeats):
-            ms, its, ran = _timed_solve(sim, v, iters)
-            ms_list.append(ms / max(1, its))
+        try:
+            for _ in range(repeats):
+                ms, its, ran = _timed_solve(sim, v, iters)
+                ms_list.append(ms / max(1, its))
+        except RuntimeError as e:
+            # a trial whose solve stopped (a bounded device wait ran out)
+            # is left out; the state is restored below
+            failed.append({"variant": tuple(v), "error": str(e)})
+            ran = None
         sim.S["P"].copy_(P0)
         if ran is None or ran[0] == 0 or ran in seen:
             continue   # the plain-load sweep ran, or a variant already timed
@@ -89,10 +96,13 @@ def tune_sweep(sim, iters=64, repeats=3, variants=VARIANTS, cache=True):
     torch.cuda.synchronize()
     if not trials:
         M.sweep_variant = (0, 0, 0)
-        return {"variant": (0, 0, 0), "trials": [], "note": "no staged variant fits this grid"}
+        return {"variant": (0, 0, 0), "trials": [], "failed": failed,
+                "note": "no staged variant fits this grid"}
     best = min(trials, key=lambda t: t["us_per_iteration"])
     rec = {"variant": (best["chunk"], best["ring"], best["pipes"]),
            "us_per_iteration": best["us_per_iteration"], "iters": iters, "trials": trials}
+    if failed:
+        rec["failed"] = failed
     M.sweep_variant = rec["variant"]
     if cache:
         _chosen[key] = rec

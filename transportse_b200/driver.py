@@ -144,6 +144,21 @@ class Simulation:
             T = numpy.moveaxis(T, 3, 0)
         self.S["T"] = torch.as_tensor(numpy.ascontiguousarray(T), **dev)
 
+    def swap_state(self, S):
+        """Make ``S`` (a dict of device tensors with the names, shapes and
+        dtypes of ``self.S``) the model's state and return the previous one.
+        A caller that streams inputs from the host can then fill one set of
+        buffers on a copy stream while the other set steps: later ``run``
+        calls read and write ``S``."""
+        if set(S) != set(self.S):
+            raise ValueError("swap_state: the state names differ")
+        for n, t in S.items():
+            o = self.S[n]
+            if t.shape != o.shape or t.dtype != o.dtype or t.device != o.device:
+                raise ValueError("swap_state: %s differs in shape, dtype or device" % n)
+        old, self.S = self.S, S
+        return old
+
     def field(self, name):
         """One field as a NumPy array in the reference layout."""
         t = self.S[name].detach().cpu().numpy()
