@@ -50,6 +50,7 @@ struct BatchItem {
     TseSolveStatus* status;
     double* X_out;
     long long cells;
+    int nparts;   // > 0: the setup wrote the first cycle (records, r', x^2 partials)
 };
 
 struct BatchShared {
@@ -767,10 +768,12 @@ static int run_fused(std::vector<BatchItem<Form>>& v, TseDcOptions* opts, void* 
         per_sm < 1)
         return TSE_ERR_LAUNCH;
 
-    // every model: state, scaled records, first residual
+    // every model: state, scaled records, first residual (written by a fused
+    // setup, which leaves the x^2 total)
     for (auto& it : v) {
-        int rc = dc_begin(it.F, it.c, it.dt, stream);
-        if (rc == TSE_OK) rc = dc_residual(it.F, it.c, stream);
+        int rc = it.nparts > 0 ? dc_begin_fused(it.c, it.dt, it.nparts, stream)
+                               : dc_begin(it.F, it.c, it.dt, stream);
+        if (rc == TSE_OK && it.nparts == 0) rc = dc_residual(it.F, it.c, stream);
         if (rc != TSE_OK) return rc;
     }
     std::vector<int> active(n), inner(n, 0);
@@ -1536,8 +1539,9 @@ static int run_fused_graph(std::vector<BatchItem<Form>>& v, TseDcOptions* opts, 
     // every model: state, scaled records, first residual (as run_fused)
     int rc = TSE_OK;
     for (auto& it : v) {
-        rc = dc_begin(it.F, it.c, it.dt, stream);
-        if (rc == TSE_OK) rc = dc_residual(it.F, it.c, stream);
+        rc = it.nparts > 0 ? dc_begin_fused(it.c, it.dt, it.nparts, stream)
+                           : dc_begin(it.F, it.c, it.dt, stream);
+        if (rc == TSE_OK && it.nparts == 0) rc = dc_residual(it.F, it.c, stream);
         if (rc != TSE_OK) break;
     }
     std::vector<FusedModel> hm(n);
@@ -1639,6 +1643,8 @@ extern "C" int32_t tse_compute_P_dc_batch(const TseBatchPressure* items, int32_t
     if (!items || n < 1 || !d_batch_ws) return TSE_ERR_ARG;
     cudaStream_t stream = (cudaStream_t)stream_;
     std::vector<BatchItem<PressureForm>> v(n);
+    // the cluster form scales and forms the first residual in its own kernel
+    const bool fused = !(opts && opts->max_blocks > 0);
     for (int i = 0; i < n; ++i) {
         const TseBatchPressure& b = items[i];
         const TsePressureArgs* a = b.args;
@@ -1646,7 +1652,9 @@ extern "C" int32_t tse_compute_P_dc_batch(const TseBatchPressure* items, int32_t
             !finite_dt(a->dt_P, a->min_dt) || !a->P)
             return TSE_ERR_ARG;
         PressureSetup S;
-        int rc = setup_pressure(b.grid, a, b.d_workspace, b.workspace_bytes, stream, S);
+        int np = 0;
+        int rc = fused ? setup_pressure_dc(b.grid, a, b.d_workspace, b.workspace_bytes, stream, S, &np)
+                         : setup_pressure(b.grid, a, b.d_workspace, b.workspace_bytes, stream, S);
         if (rc != TSE_OK) return rc;
         if (S.tail_bytes < dc_extra_bytes(S.L)) return TSE_ERR_WORKSPACE;
         v[i].F = S.F;
@@ -1656,6 +1664,7 @@ extern "C" int32_t tse_compute_P_dc_batch(const TseBatchPressure* items, int32_t
         v[i].status = b.d_status;
         v[i].X_out = a->P;
         v[i].cells = 2 * S.L.Nc;
+        v[i].nparts = np;
     }
     if (opts && opts->max_blocks > 0) return launch_batch(v, opts, d_batch_ws, batch_ws_bytes, stream);
     const int g = run_fused_graph(v, opts, d_batch_ws, batch_ws_bytes, stream);
@@ -1670,6 +1679,7 @@ extern "C" int32_t tse_compute_C_dc_batch(const TseBatchSpecies* items, int32_t 
     if (!items || n < 1 || !d_batch_ws) return TSE_ERR_ARG;
     cudaStream_t stream = (cudaStream_t)stream_;
     std::vector<BatchItem<TransportForm>> v(n);
+    const bool fused = !(opts && opts->max_blocks > 0);
     for (int i = 0; i < n; ++i) {
         const TseBatchSpecies& b = items[i];
         const TseSpeciesArgs* a = b.args;
@@ -1677,7 +1687,9 @@ extern "C" int32_t tse_compute_C_dc_batch(const TseBatchSpecies* items, int32_t 
             !finite_dt(a->dt, a->min_dt) || !a->C)
             return TSE_ERR_ARG;
         TransportSetup S;
-        int rc = setup_species(b.grid, a, b.d_workspace, b.workspace_bytes, stream, S);
+        int np = 0;
+        int rc = fused ? setup_species_dc(b.grid, a, b.d_workspace, b.workspace_bytes, stream, S, &np)
+                         : setup_species(b.grid, a, b.d_workspace, b.workspace_bytes, stream, S);
         if (rc != TSE_OK) return rc;
         if (S.tail_bytes < dc_extra_bytes(S.L)) return TSE_ERR_WORKSPACE;
         v[i].F = S.F;
@@ -1688,6 +1700,7 @@ extern "C" int32_t tse_compute_C_dc_batch(const TseBatchSpecies* items, int32_t 
         v[i].status = b.d_status;
         v[i].X_out = a->C;
         v[i].cells = 2 * S.L.Nc;
+        v[i].nparts = np;
     }
     if (opts && opts->max_blocks > 0) return launch_batch(v, opts, d_batch_ws, batch_ws_bytes, stream);
     const int g = run_fused_graph(v, opts, d_batch_ws, batch_ws_bytes, stream);
@@ -1702,6 +1715,7 @@ extern "C" int32_t tse_compute_T_dc_batch(const TseBatchHeat* items, int32_t n,
     if (!items || n < 1 || !d_batch_ws) return TSE_ERR_ARG;
     cudaStream_t stream = (cudaStream_t)stream_;
     std::vector<BatchItem<TransportForm>> v(n);
+    const bool fused = !(opts && opts->max_blocks > 0);
     for (int i = 0; i < n; ++i) {
         const TseBatchHeat& b = items[i];
         const TseHeatArgs* a = b.args;
@@ -1709,7 +1723,9 @@ extern "C" int32_t tse_compute_T_dc_batch(const TseBatchHeat* items, int32_t n,
             !finite_dt(a->dt, a->min_dt) || !a->T)
             return TSE_ERR_ARG;
         TransportSetup S;
-        int rc = setup_heat(b.grid, a, b.d_workspace, b.workspace_bytes, stream, S);
+        int np = 0;
+        int rc = fused ? setup_heat_dc(b.grid, a, b.d_workspace, b.workspace_bytes, stream, S, &np)
+                         : setup_heat(b.grid, a, b.d_workspace, b.workspace_bytes, stream, S);
         if (rc != TSE_OK) return rc;
         if (S.tail_bytes < dc_extra_bytes(S.L)) return TSE_ERR_WORKSPACE;
         v[i].F = S.F;
@@ -1720,6 +1736,7 @@ extern "C" int32_t tse_compute_T_dc_batch(const TseBatchHeat* items, int32_t n,
         v[i].status = b.d_status;
         v[i].X_out = a->T;
         v[i].cells = 2 * S.L.Nc;
+        v[i].nparts = np;
     }
     if (opts && opts->max_blocks > 0) return launch_batch(v, opts, d_batch_ws, batch_ws_bytes, stream);
     const int g = run_fused_graph(v, opts, d_batch_ws, batch_ws_bytes, stream);

@@ -830,6 +830,16 @@ int dc_apply(const DcCtl& c, cudaStream_t stream) {
     return cudaGetLastError() == cudaSuccess ? TSE_OK : TSE_ERR_LAUNCH;
 }
 
+int dc_begin_fused(const DcCtl& c, double dt, int nparts, cudaStream_t stream) {
+    float* dbase = c.D[0] - dc_margin(c.L);
+    const long long dlen = dc_delta_len(c.L, c.Ncal);
+    if (cudaMemsetAsync(dbase, 0, (size_t)2 * dlen * sizeof(float), stream) != cudaSuccess)
+        return TSE_ERR_LAUNCH;
+    dc_init_state_kernel<<<1, 1, 0, stream>>>(c.st, dt);
+    dc_x2_kernel<<<1, kBlock, 0, stream>>>(c, nparts);
+    return cudaGetLastError() == cudaSuccess ? TSE_OK : TSE_ERR_LAUNCH;
+}
+
 int dc_finish(const DcCtl& c, TseSolveStatus* d_status, double* X_out, cudaStream_t stream) {
     dc_status_kernel<<<1, 1, 0, stream>>>(c.st, d_status);
     if (cudaGetLastError() != cudaSuccess) return TSE_ERR_LAUNCH;
@@ -858,10 +868,11 @@ extern "C" int32_t tse_compute_P_dc(const TseGrid* grid, const TsePressureArgs* 
         return TSE_ERR_ARG;
     cudaStream_t stream = (cudaStream_t)stream_;
     PressureSetup S;
-    int rc = setup_pressure(grid, args, d_ws, ws_bytes, stream, S);
+    int nparts = 0;
+    int rc = setup_pressure_dc(grid, args, d_ws, ws_bytes, stream, S, &nparts);
     if (rc != TSE_OK) return rc;
     return run_dc(S, args->dt_P, args->inc_it, args->max_dt, args->min_dt, args->P_conv,
-                  args->max_it, 1, 0, opts, args->SOR, PA_P, args->P, d_status, stream);
+                  args->max_it, 1, 0, opts, args->SOR, PA_P, args->P, d_status, stream, nparts);
 }
 
 extern "C" int32_t tse_compute_C_dc(const TseGrid* grid, const TseSpeciesArgs* a,

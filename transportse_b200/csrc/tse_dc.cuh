@@ -164,6 +164,35 @@ template <class Form>
 int dc_halve(const Form& F, const DcCtl& c, cudaStream_t stream);
 int dc_apply(const DcCtl& c, cudaStream_t stream);
 int dc_finish(const DcCtl& c, TseSolveStatus* d_status, double* X_out, cudaStream_t stream);
+// the start of a solve whose setup was fused (setup_*_dc): state record,
+// zeroed corrections, the x^2 total of the setup's nparts partials
+int dc_begin_fused(const DcCtl& c, double dt, int nparts, cudaStream_t stream);
+
+// The mixed-precision form's first correction cycle, written by the
+// assembly pass of a solve: per colour the FP32 record K'_q = k_q / Den and
+// r' = (sum(x) - Den x) / Den of the initial iterate (sum() in the form's
+// order), and per block the sum of x^2.  No bit-exactness is claimed for
+// this form: 1/Den is formed once.
+struct DcFuse {
+    float* K[2];
+    long long Ncal;
+    double* partials;
+    int per_thread;   // cells a thread assembles (blocks of kBlock consecutive cells)
+};
+
+// Assembly grid of a fused setup: a function of the grid alone (at most
+// kMaxBlocks blocks), so the x^2 sums are grouped the same way on every device.
+inline void dc_fuse_grid(const Layout& L, long long& per, long long& nb) {
+    const long long total = (long long)L.nx * L.ny * L.nzp;
+    const long long groups = (total + kBlock - 1) / kBlock;
+    per = (groups + kMaxBlocks - 1) / kMaxBlocks;
+    nb = (groups + per - 1) / per;
+}
+
+// Pressure setup for the mixed-precision form (tse_pressure.cu): the exact
+// form's arrays plus the first cycle's records, r' and *nparts x^2 partials.
+int setup_pressure_dc(const TseGrid* grid, const TsePressureArgs* args, void* d_ws, size_t ws_bytes,
+                      cudaStream_t stream, PressureSetup& S, int* nparts);
 
 // Transport setups for the mixed-precision form (tse_transport.cu): the
 // exact form's arrays plus, from the same pass, the FP32 records, r' of the

@@ -12,6 +12,7 @@
 // reference's.  Compiled with --fmad=false.
 #include <atomic>
 
+#include "tse_dc.cuh"
 #include "tse_forms.cuh"
 #include "tse_rbsolve.cuh"
 #include "tse_rbsolve_tma.cuh"
@@ -26,11 +27,15 @@ __device__ __forceinline__ double alpha_(double K1, double K2, double n1, double
            harm2(r1, r2, d1, d2);
 }
 
-__global__ void assemble_p_kernel(TseGrid g, TsePressureArgs a, PressureForm F, uint8_t* mask0,
-                                  uint8_t* mask1, Layout L) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long total = (long long)L.nx * L.ny * L.nzp;
-    if (t >= total) return;
+// One cell of the pressure assembly (cell t of the padded natural order);
+// with fz, also the mixed-precision form's first cycle (DcFuse): K'_q =
+// k_q / Den and r' = (sum(Pn) - Den Pn) / Den with sum() of PressureForm over
+// the neighbours' Pn; returns Pn^2 (0 for padding).
+template <bool DC>
+__device__ __forceinline__ double assemble_p_cell(const TseGrid& g, const TsePressureArgs& a,
+                                                  const PressureForm& F, uint8_t* mask0,
+                                                  uint8_t* mask1, const Layout& L, long long t,
+                                                  const DcFuse& fz) {
     const int nx = L.nx, ny = L.ny, nz = L.nz;
     int i, j, k;
     long long row;
@@ -43,7 +48,12 @@ __global__ void assemble_p_kernel(TseGrid g, TsePressureArgs a, PressureForm F, 
     if (k >= nz) {
         for (int q = 0; q < PA_COUNT; ++q) b[q * N + m] = 0.0;
         msk[m] = 0;
-        return;
+        if (DC) {
+            float2* rec = reinterpret_cast<float2*>(fz.K[col] + 6 * m);
+            for (int q = 0; q < 3; ++q) rec[q] = make_float2(0.0f, 0.0f);
+            fz.K[col][6 * fz.Ncal + m] = 0.0f;
+        }
+        return 0.0;
     }
     const long long c = row * nz + k;
     const long long sx = (long long)ny * nz;
@@ -83,6 +93,8 @@ __global__ void assemble_p_kernel(TseGrid g, TsePressureArgs a, PressureForm F, 
     const double R = S / a.dt_P;
     const double M = A_ + C_ + E_ + G_ + I_ + K_;
     const double pn = a.P[c];
+    const double AB = A_ * B_, CD = C_ * D_, IJ = I_ * J_, KL = K_ * L_, RPN = R * pn, WP = a.WP[c];
+    const double DEN = R + M;
     a.Pn[c] = pn;
     b[PA_A * N + m] = A_;
     b[PA_C * N + m] = C_;
@@ -90,20 +102,79 @@ __global__ void assemble_p_kernel(TseGrid g, TsePressureArgs a, PressureForm F, 
     b[PA_G * N + m] = G_;
     b[PA_I * N + m] = I_;
     b[PA_K * N + m] = K_;
-    b[PA_AB * N + m] = A_ * B_;
-    b[PA_CD * N + m] = C_ * D_;
-    b[PA_IJ * N + m] = I_ * J_;
-    b[PA_KL * N + m] = K_ * L_;
-    b[PA_RPN * N + m] = R * pn;
-    b[PA_WP * N + m] = a.WP[c];
-    b[PA_DEN * N + m] = R + M;
+    b[PA_AB * N + m] = AB;
+    b[PA_CD * N + m] = CD;
+    b[PA_IJ * N + m] = IJ;
+    b[PA_KL * N + m] = KL;
+    b[PA_RPN * N + m] = RPN;
+    b[PA_WP * N + m] = WP;
+    b[PA_DEN * N + m] = DEN;
     b[PA_S * N + m] = S;
     b[PA_M * N + m] = M;
     b[PA_PN * N + m] = pn;
     b[PA_P * N + m] = pn;
     uint8_t f = neighbour_flags(i, j, k, nx, ny, nz);
-    if (!(a.BP[c] != 0.0)) f |= F_ACTIVE;
+    const bool active = !(a.BP[c] != 0.0);
+    if (active) f |= F_ACTIVE;
     msk[m] = f;
+    if (DC) {
+        float2* rec = reinterpret_cast<float2*>(fz.K[col] + 6 * m);
+        float rp = 0.0f;
+        if (active) {
+            const double rden = 1.0 / DEN;
+            rec[0] = make_float2((float)(A_ * rden), (float)(C_ * rden));
+            rec[1] = make_float2((float)(E_ * rden), (float)(G_ * rden));
+            rec[2] = make_float2((float)(I_ * rden), (float)(K_ * rden));
+            const double* P = a.P;
+            const double s = F.sum_with(
+                [&](int q) -> double {
+                    switch (q) {
+                        case PA_A: return A_;
+                        case PA_C: return C_;
+                        case PA_E: return E_;
+                        case PA_G: return G_;
+                        case PA_I: return I_;
+                        case PA_K: return K_;
+                        case PA_AB: return AB;
+                        case PA_CD: return CD;
+                        case PA_IJ: return IJ;
+                        case PA_KL: return KL;
+                        case PA_RPN: return RPN;
+                        default: return WP;
+                    }
+                },
+                [&](int q) -> double {
+                    return q == 0 ? P[c + sx] : q == 1 ? P[c - sx] : q == 2 ? P[c + nz]
+                         : q == 3 ? P[c - nz] : q == 4 ? P[c + 1] : P[c - 1];
+                },
+                f);
+            rp = (float)((s - DEN * pn) * rden);
+        } else {
+            for (int q = 0; q < 3; ++q) rec[q] = make_float2(0.0f, 0.0f);
+        }
+        fz.K[col][6 * fz.Ncal + m] = rp;
+    }
+    return pn * pn;
+}
+
+template <bool DC>
+__global__ void assemble_p_kernel(TseGrid g, TsePressureArgs a, PressureForm F, uint8_t* mask0,
+                                  uint8_t* mask1, Layout L, DcFuse fz) {
+    const long long total = (long long)L.nx * L.ny * L.nzp;
+    if (!DC) {
+        const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        if (t < total) assemble_p_cell<false>(g, a, F, mask0, mask1, L, t, fz);
+        return;
+    }
+    __shared__ double sh[kBlock / 32];
+    double x2 = 0.0;
+    for (int s = 0; s < fz.per_thread; ++s) {
+        const long long t = ((long long)blockIdx.x * fz.per_thread + s) * kBlock + threadIdx.x;
+        if (t >= total) break;
+        x2 = x2 + assemble_p_cell<true>(g, a, F, mask0, mask1, L, t, fz);
+    }
+    const double bs = block_sum<kBlock>(x2, sh);
+    if (threadIdx.x == 0) fz.partials[blockIdx.x] = bs;
 }
 
 // compact colour arrays -> natural (nx, ny, nz) layout
@@ -132,8 +203,8 @@ size_t pressure_ws_bytes(const Layout& L, long long* Ncal_out) {
 // Carve the workspace and launch the assembly (shared by the exact and the
 // defect-correction pressure solves).  The bytes after the exact form's
 // arrays are returned in `tail` for the caller's own use.
-int setup_pressure(const TseGrid* grid, const TsePressureArgs* args, void* d_ws, size_t ws_bytes,
-                   cudaStream_t stream, PressureSetup& S) {
+static int carve_pressure(const TseGrid* grid, const TsePressureArgs* args, void* d_ws,
+                          size_t ws_bytes, cudaStream_t stream, PressureSetup& S) {
     S.L = make_layout(grid->nx, grid->ny, grid->nz);
     const size_t need = pressure_ws_bytes(S.L, &S.Ncal);
     if (need > ws_bytes) return TSE_ERR_WORKSPACE;
@@ -158,9 +229,37 @@ int setup_pressure(const TseGrid* grid, const TsePressureArgs* args, void* d_ws,
     S.tail = (char*)d_ws + need;
     S.tail_bytes = ws_bytes - need;
     if (cudaMemsetAsync(S.bar, 0, sizeof(GridBarrier), stream) != cudaSuccess) return TSE_ERR_LAUNCH;
+    return TSE_OK;
+}
+
+int setup_pressure(const TseGrid* grid, const TsePressureArgs* args, void* d_ws, size_t ws_bytes,
+                   cudaStream_t stream, PressureSetup& S) {
+    int rc = carve_pressure(grid, args, d_ws, ws_bytes, stream, S);
+    if (rc != TSE_OK) return rc;
     const long long total = (long long)S.L.nx * S.L.ny * S.L.nzp;
-    assemble_p_kernel<<<(unsigned)((total + kBlock - 1) / kBlock), kBlock, 0, stream>>>(
-        *grid, *args, S.F, S.mask[0], S.mask[1], S.L);
+    assemble_p_kernel<false><<<(unsigned)((total + kBlock - 1) / kBlock), kBlock, 0, stream>>>(
+        *grid, *args, S.F, S.mask[0], S.mask[1], S.L, DcFuse{});
+    return cudaGetLastError() == cudaSuccess ? TSE_OK : TSE_ERR_LAUNCH;
+}
+
+int setup_pressure_dc(const TseGrid* grid, const TsePressureArgs* args, void* d_ws, size_t ws_bytes,
+                      cudaStream_t stream, PressureSetup& S, int* nparts) {
+    int rc = carve_pressure(grid, args, d_ws, ws_bytes, stream, S);
+    if (rc != TSE_OK) return rc;
+    if (S.tail_bytes < dc_extra_bytes(S.L)) return TSE_ERR_WORKSPACE;
+    DcCtl c;
+    dc_carve(S, c, PA_P);
+    long long per, nb;
+    dc_fuse_grid(S.L, per, nb);
+    DcFuse fz;
+    fz.K[0] = c.K[0];
+    fz.K[1] = c.K[1];
+    fz.Ncal = c.Ncal;
+    fz.partials = S.partials;
+    fz.per_thread = (int)per;
+    assemble_p_kernel<true><<<(unsigned)nb, kBlock, 0, stream>>>(*grid, *args, S.F, S.mask[0],
+                                                                  S.mask[1], S.L, fz);
+    *nparts = (int)nb;
     return cudaGetLastError() == cudaSuccess ? TSE_OK : TSE_ERR_LAUNCH;
 }
 

@@ -329,19 +329,9 @@ __device__ __forceinline__ void store_padding(const TransportForm& F, uint8_t* m
     msk[x.m] = 0;
 }
 
-// The mixed-precision form's first correction cycle, written by the same
-// pass: per colour the FP32 record K'_q = omega co_q / Den and
-// r' = (sum(Xn) - Den Xn) / Den of the initial iterate (sum() in
-// TransportForm's order; the neighbour products are the assembly's own
-// co_q * Xn_q), and per block the sum of Xn^2.  No bit-exactness is claimed
-// for this form: 1/Den is formed once.
-struct DcFuse {
-    float* K[2];
-    long long Ncal;
-    double* partials;
-    int per_thread;   // cells a thread assembles (blocks of kBlock consecutive cells)
-};
-
+// The first correction cycle of the mixed-precision form (DcFuse): K'_q =
+// omega co_q / Den, and r' with sum() of TransportForm, whose neighbour
+// products are the assembly's own co_q * Xn_q.
 __device__ __forceinline__ void store_dc(const TransportForm& F, const DcFuse& fz, const CellIdx& x,
                                          const TransportTerms* T) {
     float* Kc = fz.K[x.col];
@@ -510,9 +500,7 @@ static int setup_transport(const TseGrid* grid, const Args* a, void* d_ws, size_
 }
 
 // carve + the assembly that also writes the mixed-precision form's first
-// cycle (records, r', x^2 partials); *nparts: the number of partials.  The
-// block count is a function of the grid alone (at most kMaxBlocks), so the
-// x^2 sums are grouped the same way on every device.
+// cycle (records, r', x^2 partials); *nparts: the number of partials
 template <class Args, class AssembleK>
 static int setup_transport_dc(const TseGrid* grid, const Args* a, void* d_ws, size_t ws_bytes,
                               cudaStream_t stream, AssembleK kernel, int imbl, TransportSetup& S,
@@ -522,10 +510,8 @@ static int setup_transport_dc(const TseGrid* grid, const Args* a, void* d_ws, si
     if (S.tail_bytes < dc_extra_bytes(S.L)) return TSE_ERR_WORKSPACE;
     DcCtl c;
     dc_carve(S, c, TA_X);
-    const long long total = (long long)S.L.nx * S.L.ny * S.L.nzp;
-    const long long groups = (total + kBlock - 1) / kBlock;
-    const long long per = (groups + kMaxBlocks - 1) / kMaxBlocks;
-    const long long nb = (groups + per - 1) / per;
+    long long per, nb;
+    dc_fuse_grid(S.L, per, nb);
     DcFuse fz;
     fz.K[0] = c.K[0];
     fz.K[1] = c.K[1];
