@@ -571,7 +571,8 @@ def e2e_steps(ctx, sim, steps):
         sim.swap_state(bufs[0])
     ms, upd = ctx.max_sum(f0.elapsed_time(f1), sum(M.cell_updates[k] - cu[k] for k in cu))
     return {"value": upd / (ms / 1e3), "unit": "cell-updates/s", "h2d_bytes_per_step": int(h2d),
-            "d2h_bytes_per_step": int(d2h), "copies": "copy stream, double-buffered state"}
+            "d2h_bytes_per_step": int(d2h), "copies": "copy stream, double-buffered state",
+            "step": "the first time step from the host inputs, every step"}
 
 
 def roofline(res, precision, peak, peak_kind):

@@ -22,8 +22,10 @@
 // copies, or, where its stages do not fit, dc_sweep_kernel (48 registers,
 // 5 blocks per SM, plain loads).  The FP64 residual, the x += d update and the dt
 // halving (reset + new R terms) are separate, ordinary kernels, so their
-// register appetite does not limit the sweeps' occupancy.  The host reads one
-// small state record per correction cycle.
+// register appetite does not limit the sweeps' occupancy; the first cycle's
+// records, residual and x^2 come from the assembly pass itself (setup_*_dc),
+// and the last x += d is fused with the unpack.  The host reads one small
+// state record per correction cycle.
 //
 // An inner cell-update streams the six FP32 coefficients (one 24-byte record),
 // r' and the flag byte from DRAM -- 29 bytes; d and the neighbours' d stay in
