@@ -1467,7 +1467,7 @@ static int run_fused_graph(std::vector<BatchItem<Form>>& v, TseDcOptions* opts, 
     if (nb > (long long)nch_max) nb = (long long)nch_max;
     const unsigned grid_small = (unsigned)(4 * sms), grid_big = (unsigned)(8 * sms);
 
-    // the graph: one WHILE node, its body captured from the stream.  Its
+    // the graph: one WHILE node, its body built node by node.  Its
     // nodes hold only workspace addresses, launch shapes and the stage
     // layout, all fixed by the key, so a later call with the same key reuses
     // the instantiated graph (the models' data go in through the workspace)
@@ -1490,35 +1490,56 @@ static int run_fused_graph(std::vector<BatchItem<Form>>& v, TseDcOptions* opts, 
             built = cudaGraphAddNode(&node, graph, nullptr, 0, &cp) == cudaSuccess;
             if (built) body = cp.conditional.phGraph_out[0];
         }
-        if (built)
-            built = cudaStreamBeginCaptureToGraph(stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed) ==
+        // The body, node by node (no stream capture: a capture in progress
+        // would stand in the way of other threads' work on their own
+        // streams, e.g. a model's state going up from pageable memory): the
+        // loop's kernels in order, the sweep a cooperative launch.
+        cudaGraphNode_t prev = nullptr;
+        auto add = [&](const void* func, unsigned grid, unsigned block, size_t shmem, void** kargs,
+                       bool coop) {
+            if (!built) return;
+            cudaKernelNodeParams kp = {};
+            kp.func = const_cast<void*>(func);
+            kp.gridDim = dim3(grid);
+            kp.blockDim = dim3(block);
+            kp.sharedMemBytes = (unsigned)shmem;
+            kp.kernelParams = kargs;
+            kp.extra = nullptr;
+            cudaGraphNode_t node;
+            built = cudaGraphAddKernelNode(&node, body, prev ? &prev : nullptr, prev ? 1 : 0, &kp) ==
                     cudaSuccess;
-        if (built) {
-            fused_plan_kernel<<<1, kPlanThreads, 0, stream>>>(d_ctl, d_models, d_items, d_idx, d_args, d_chunks,
-                                                              d_cpart, d_any, d_bar);
-            fused_fill_kernel<<<grid_small, kBlock, 0, stream>>>(d_args, d_chunks);
-            cudaLaunchConfig_t lc = {};
-            lc.gridDim = dim3((unsigned)nb);
-            lc.blockDim = dim3((unsigned)fused_threads);
-            lc.dynamicSmemBytes = smem;
-            lc.stream = stream;
-            cudaLaunchAttribute at[1];
-            at[0].id = cudaLaunchAttributeCooperative;
-            at[0].val.cooperative = 1;
-            lc.attrs = at;
-            lc.numAttrs = 1;
-            const FusedArgs* a_ptr = d_args;
-            FusedCtl* c_ptr = d_ctl;
-            void* kargs[] = {(void*)&a_ptr, (void*)&T, (void*)&c_ptr};
-            const cudaError_t le = cudaLaunchKernelExC(&lc, kernel, kargs);
-            fused_events_kernel<<<1, kPlanThreads, 0, stream>>>(d_ctl, d_models, d_args, d_idx, d_act, d_rstart,
-                                                                cond);
-            fused_update_kernel<Form><<<grid_big, kBlock, 0, stream>>>(d_args, d_forms, d_idx, d_act);
-            fused_residual_kernel<Form><<<grid_big, kBlock, 0, stream>>>(d_args, d_forms, d_idx, d_rstart, d_ctl);
-            fused_x2_kernel<<<grid_small, kBlock, 0, stream>>>(d_args, d_act);
-            const cudaError_t ce = cudaStreamEndCapture(stream, &body);
-            built = le == cudaSuccess && ce == cudaSuccess && cudaGetLastError() == cudaSuccess;
-        }
+            if (built && coop) {
+                cudaKernelNodeAttrValue v = {};
+                v.cooperative = 1;
+                built = cudaGraphKernelNodeSetAttribute(node, cudaKernelNodeAttributeCooperative, &v) ==
+                        cudaSuccess;
+            }
+            prev = node;
+        };
+        const FusedCtl* c_ctl = d_ctl;
+        const FusedArgs* c_args = d_args;
+        const int* c_idx = d_idx;
+        const int* c_act = d_act;
+        const long long* c_rstart = d_rstart;
+        const Form* c_forms = d_forms;
+        FusedCtl* m_ctl = d_ctl;
+        void* a_plan[] = {(void*)&c_ctl, (void*)&d_models, (void*)&d_items, (void*)&d_idx, (void*)&d_args,
+                          (void*)&d_chunks, (void*)&d_cpart, (void*)&d_any, (void*)&d_bar};
+        void* a_fill[] = {(void*)&c_args, (void*)&d_chunks};
+        void* a_sweep[] = {(void*)&c_args, (void*)&T, (void*)&m_ctl};
+        void* a_events[] = {(void*)&m_ctl, (void*)&d_models, (void*)&c_args, (void*)&c_idx, (void*)&d_act,
+                            (void*)&d_rstart, (void*)&cond};
+        void* a_update[] = {(void*)&c_args, (void*)&c_forms, (void*)&c_idx, (void*)&c_act};
+        void* a_resid[] = {(void*)&c_args, (void*)&c_forms, (void*)&c_idx, (void*)&c_rstart, (void*)&c_ctl};
+        void* a_x2[] = {(void*)&c_args, (void*)&c_act};
+        add((const void*)fused_plan_kernel, 1, kPlanThreads, 0, a_plan, false);
+        add((const void*)fused_fill_kernel, grid_small, kBlock, 0, a_fill, false);
+        add(kernel, (unsigned)nb, (unsigned)fused_threads, smem, a_sweep, true);
+        add((const void*)fused_events_kernel, 1, kPlanThreads, 0, a_events, false);
+        add((const void*)fused_update_kernel<Form>, grid_big, kBlock, 0, a_update, false);
+        add((const void*)fused_residual_kernel<Form>, grid_big, kBlock, 0, a_resid, false);
+        add((const void*)fused_x2_kernel, grid_small, kBlock, 0, a_x2, false);
+        if (!built) cudaGetLastError();
         if (built) built = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
         if (!built) {
             cudaGetLastError();
