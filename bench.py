@@ -88,7 +88,8 @@ def parse_args():
                          "solves (one fused launch per solve kind, the default)")
     ap.add_argument("--requests", type=int, default=40, help="serving: requests")
     ap.add_argument("--rate", type=float, default=20.0, help="serving: arrivals per second")
-    ap.add_argument("--slots", type=int, default=8, help="serving: concurrent models")
+    ap.add_argument("--slots", type=int, default=0,
+                    help="serving: requests running at once (0: no limit, admission by the HBM budget)")
     ap.add_argument("--gate", choices=("eager", "lockstep"), default="lockstep",
                     help="serving, batched: issue a batch as soon as a solve waits and the GPU "
                          "is free (eager), or once every running request waits (lockstep)")
@@ -258,7 +259,7 @@ def bench_sloped(a):
         "mass_rel_diff_vs_fp64": mass_rel}))
 
 
-def serving_run(a, dev, requests, steps, nmax, rate=20.0, slots=8, clocks=True):
+def serving_run(a, dev, requests, steps, nmax, rate=20.0, slots=0, clocks=True):
     """Poisson arrivals of cubic-grid simulations (log-uniform edge 16-nmax),
     each ``steps`` coupled flow/heat/species steps; HBM-budget admission,
     state resident on the device, continuous batching of the running
@@ -281,8 +282,10 @@ def serving_run(a, dev, requests, steps, nmax, rate=20.0, slots=8, clocks=True):
     return {
         "metric": "SOR cell-updates/s", "value": st["cell_updates_per_s"], "unit": "cell-updates/s",
         "config": {"workload": "serving: %d Poisson arrivals at %.0f/s, cubic n log-uniform 16-%d, "
-                               "%d steps each, %d slots, HBM budget %.0f GB"
-                               % (requests, rate, nmax, steps, slots, budget / 1e9),
+                               "%d steps each, %s, HBM budget %.0f GB"
+                               % (requests, rate, nmax, steps,
+                                  "%d slots" % slots if slots else "admission by the budget alone",
+                                  budget / 1e9),
                    "requests": requests, "steps": steps},
         "latency_p50_s": st["p50_s"], "latency_p99_s": st["p99_s"], "latency_mean_s": st["mean_s"],
         "makespan_s": st["makespan_s"], "cell_updates": st["cell_updates"],

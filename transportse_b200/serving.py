@@ -58,15 +58,18 @@ class Server:
 
     def __init__(self, device=None, slots=8, hbm_budget=None, precision="fp32dc", max_blocks=None,
                  keep=("P", "C", "T"), batched=None, cluster=0, eager=False):
+        """``slots``: requests running at once; 0 or None: no limit, a request
+        starts as soon as it has arrived and its state fits the HBM budget
+        (admission by the budget alone)."""
         self.device = torch.device(device if device is not None else "cuda")
-        self.slots = max(1, int(slots))
+        self.slots = max(0, int(slots or 0))
         self.batched = (precision == "fp32dc") if batched is None else bool(batched)
         if self.batched and precision != "fp32dc":
             raise ValueError("batched solves need precision='fp32dc'")
         self.gate = BatchGate(self.device, cluster=cluster, eager=eager) if self.batched else None
         self.budget = HbmBudget(hbm_budget if hbm_budget is not None else default_budget(self.device))
         self.precision = precision
-        self.max_blocks = max_blocks if max_blocks else block_cap(self.device, self.slots)
+        self.max_blocks = max_blocks if max_blocks else block_cap(self.device, max(1, self.slots))
         self.keep = keep
         self.pending = []          # heap of (arrival, rid, request)
         self.cv = threading.Condition()
@@ -81,9 +84,12 @@ class Server:
     def start(self):
         self.t0 = time.perf_counter()
         for _ in range(self.slots):
-            th = threading.Thread(target=self._worker, daemon=True)
-            th.start()
-            self.workers.append(th)
+            self._spawn()
+
+    def _spawn(self):
+        th = threading.Thread(target=self._worker, daemon=True)
+        th.start()
+        self.workers.append(th)
 
     def submit(self, req):
         req.bytes = state_bytes(req.config, self.precision)
@@ -93,6 +99,10 @@ class Server:
         with self.cv:
             heapq.heappush(self.pending, (req.arrival, req.rid, req))
             self.cv.notify()
+        if self.slots == 0:
+            # no slot limit: a worker for every request, held back only by
+            # the budget
+            self._spawn()
         return req
 
     def cancel(self, rid):
@@ -170,7 +180,7 @@ class Server:
                       "p99_s": float(numpy.percentile(lat, 99)), "mean_s": float(lat.mean()),
                       "makespan_s": makespan, "cell_updates": updates,
                       "cell_updates_per_s": updates / makespan if makespan > 0 else 0.0,
-                      "slots": self.slots, "max_blocks": self.max_blocks,
+                      "slots": self.slots or "unlimited", "max_blocks": self.max_blocks,
                       "batched": self.batched,
                       "batch": self.gate.stats() if self.gate is not None else None}
 
