@@ -75,17 +75,21 @@ def test_serving_results_alone_and_in_the_mix(cuda_device):
             assert rel_err(r.result[k], alone[k]) <= 1e-6, (r.rid, k)
 
 
-def test_serving_with_a_slot_per_request(cuda_device):
-    """Every request starts on arrival (a slot each): new models upload their
-    state from pageable host memory while the running ones' batched calls --
-    of varying model counts, so their loop graphs are built -- are in
-    flight.  Every request completes with its alone result."""
+@pytest.mark.parametrize("slots", [12, 0])
+def test_serving_with_a_slot_per_request(slots, cuda_device):
+    """Every request starts on arrival (a slot each, or no slot limit):
+    new models upload their state from pageable host memory while the
+    running ones' batched calls -- of varying model counts, so their loop
+    graphs are built -- are in flight.  Every request completes with its
+    alone result; without a limit, no more workers than requests."""
     from transportse_b200.ensemble import run_model
     from transportse_b200.serving import Server, poisson_trace
     trace = poisson_trace(12, rate=60.0, seed=11, builder=workloads.serving_request, steps=2,
                           n_min=8, n_max=24)
-    reqs, stats = Server(device=cuda_device, slots=12).replay(trace)
+    srv = Server(device=cuda_device, slots=slots)
+    reqs, stats = srv.replay(trace)
     assert stats["requests"] == 12 and all(r.error is None for r in reqs)
+    assert len(srv.workers) <= 12
     for r in reqs[:4]:
         cfg = workloads.serving_request(11 * 1000 + r.rid, n_min=8, n_max=24)
         alone = run_model(cfg, 2, cuda_device, "fp32dc", max_blocks=0)

@@ -76,6 +76,7 @@ class Server:
         self.stop = threading.Event()
         self.t0 = None
         self.workers = []
+        self.idle = 0              # no slot limit: workers free for a request not yet claimed
         self.completed = []
 
     def now(self):
@@ -98,10 +99,17 @@ class Server:
                               % (req.rid, req.bytes / 1e9))
         with self.cv:
             heapq.heappush(self.pending, (req.arrival, req.rid, req))
+            # no slot limit: the request claims an idle worker, or a new one,
+            # so every request starts once it fits the budget and finished
+            # workers take later requests rather than accumulating
+            spawn = False
+            if self.slots == 0:
+                if self.idle > 0:
+                    self.idle -= 1
+                else:
+                    spawn = True
             self.cv.notify()
-        if self.slots == 0:
-            # no slot limit: a worker for every request, held back only by
-            # the budget
+        if spawn:
             self._spawn()
         return req
 
@@ -149,6 +157,9 @@ class Server:
                 self.budget.release(req.bytes)
                 req.finish = self.now()
                 self.completed.append(req)
+                if self.slots == 0:
+                    with self.cv:
+                        self.idle += 1
                 req.done.set()
 
     def shutdown(self):
