@@ -374,9 +374,10 @@ struct HeatKind {
 };
 
 // Both assemblies are latency-bound (FP64 divisions and neighbour loads per
-// cell).  Three 256-thread blocks per SM (80 registers) rather than the two
-// that ~96 registers allow: measured on the 256 x 256 x 128 reservoir,
-// species solves 13.6 -> 16.2 and heat solves 9.1 -> 11.5 G cell-updates/s.
+// cell).  Three 256-thread blocks per SM (80 registers, some spilled) rather
+// than the two that ~96 registers allow: measured on the 256 x 256 x 128
+// reservoir, a species solve of 5 iterations took 1.75 ms at three blocks,
+// 2.03 ms at two and 1.74 ms at four (heat, 3 iterations: 1.61, 1.90, 1.63).
 #ifndef TSE_ASM_MINB
 #define TSE_ASM_MINB 3
 #endif
