@@ -564,3 +564,37 @@ def test_batch_gate_sub_batches_by_cell_budget():
     assert B.BatchGate("cpu", batch_cells=0)._subbatches(reqs) == [reqs]
     assert B.BatchGate("cpu", cluster=8, batch_cells=1000)._subbatches(reqs) == [reqs]
     assert B.default_batch_cells("cpu") == 0
+
+
+def test_server_admission_without_and_with_a_slot_limit(monkeypatch):
+    """Serving host logic, with a stand-in for the model run (no GPU):
+    without a slot limit every request of a burst runs at once and a later
+    burst reuses the finished workers; with slots=k at most k run at once."""
+    import threading
+    import time
+
+    from transportse_b200 import serving
+    state = {"live": 0, "peak": 0}
+    lock = threading.Lock()
+
+    def fake_run(config, steps, device, precision, max_blocks, keep=(), gate=None):
+        with lock:
+            state["live"] += 1
+            state["peak"] = max(state["peak"], state["live"])
+        time.sleep(0.1)
+        with lock:
+            state["live"] -= 1
+        return {"cell_updates": 1}
+
+    monkeypatch.setattr(serving, "run_model", fake_run)
+    monkeypatch.setattr(serving, "state_bytes", lambda config, precision="fp32dc": 1)
+    trace = [(0.0, None, 1)] * 8 + [(0.5, None, 1)] * 8
+    for slots, peak, workers in ((0, 8, 8), (3, 3, 3)):
+        state.update(live=0, peak=0)
+        srv = serving.Server(device="cpu", slots=slots, hbm_budget=1 << 20, precision="fp64",
+                             max_blocks=8, batched=False)
+        reqs, st = srv.replay(trace)
+        assert st["requests"] == 16 and all(r.error is None for r in reqs)
+        assert st["cell_updates"] == 16
+        assert state["peak"] == peak, (slots, state["peak"])
+        assert len(srv.workers) == workers, (slots, len(srv.workers))

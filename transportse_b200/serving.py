@@ -19,6 +19,7 @@ aggregate cell-update rate.
 """
 from __future__ import annotations
 
+import contextlib
 import heapq
 import threading
 import time
@@ -137,8 +138,17 @@ class Server:
                 self.cv.wait(timeout=0.05)
             return heapq.heappop(self.pending)[2]
 
+    def _on_stream(self, stream):
+        """A request's context on its worker: the device and the worker's
+        own stream current (nothing to set without a CUDA device)."""
+        ctx = contextlib.ExitStack()
+        if stream is not None:
+            ctx.enter_context(torch.cuda.device(self.device))
+            ctx.enter_context(torch.cuda.stream(stream))
+        return ctx
+
     def _worker(self):
-        stream = torch.cuda.Stream(device=self.device)
+        stream = torch.cuda.Stream(device=self.device) if self.device.type == "cuda" else None
         while True:
             req = self._next()
             if req is None:
@@ -147,10 +157,11 @@ class Server:
                 return
             try:
                 req.start = self.now()
-                with torch.cuda.device(self.device), torch.cuda.stream(stream):
+                with self._on_stream(stream):
                     req.result = run_model(req.config, req.steps, self.device, self.precision,
                                            self.max_blocks, keep=self.keep, gate=self.gate)
-                    stream.synchronize()
+                    if stream is not None:
+                        stream.synchronize()
             except Exception as e:
                 req.error = e
             finally:
