@@ -195,6 +195,7 @@ struct SolveSetup {
     Form F;
     char* tail;          // workspace bytes after the exact form's arrays
     size_t tail_bytes;
+    double* faces = nullptr;   // transport: the face pass's values
 };
 using PressureSetup = SolveSetup<PressureForm>;
 using TransportSetup = SolveSetup<TransportForm>;

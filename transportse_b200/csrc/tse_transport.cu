@@ -134,28 +134,66 @@ struct AxisTerms {
     double dP, dM, minP, maxP, maxM, minM, coP, coM, oldP, oldM;
 };
 
+// The means both cells of a face form alike, computed once a face by a pass
+// before the assembly (faces_kernel): for a species harm2(D) * amean2(phi),
+// the face's value of A (tse.py:811-861); for heat the conductivity mix
+// (1 - por) lr + por lf and the mean of rho_f times that of cp_f
+// (tse.py:952-1027).  The cell on the + side forms them with the operands
+// swapped -- (d1 + d2) / (d1/H1 + d2/H2) and (X1 d1 + X2 d2) / (d1 + d2) --
+// and IEEE addition and multiplication commute, so the values are the ones
+// each cell would form itself, bit for bit.  Stored per axis for the face
+// toward the + neighbour (0 where there is none).
+__device__ __forceinline__ void species_face(const double* __restrict__ Df, const double* __restrict__ phi,
+                                             const double* __restrict__ d, long long c, long long st,
+                                             int ii, bool hp, double phic, double* __restrict__ out) {
+    double v = 0.0;
+    if (hp) {
+        const long long o = c + st;
+        const double dd = d[ii], dp = d[ii + 1];
+        const double Dc = Df[c], Dp = Df[o];
+        v = harm2w(Dp, Dc, dp, dd, dp / Dp, dd / Dc) * amean2(phi[o], phic, dp, dd);
+    }
+    out[c] = v;
+}
+
+__device__ __forceinline__ void heat_face(const TseHeatArgs& a, const double* __restrict__ d, long long c,
+                                          long long st, int ii, bool hp, double* __restrict__ k1_out,
+                                          double* __restrict__ rc_out) {
+    double k1 = 0.0, rc = 0.0;
+    if (hp) {
+        const long long o = c + st;
+        const double dd = d[ii], dp = d[ii + 1];
+        const double phic = a.phi[c], lfc = a.l_f[c], lrc = a.l_r[c], cpc = a.cp_f[c], rhc = a.rho_f[c];
+        const double php = a.phi[o], lfp = a.l_f[o], lrp = a.l_r[o], cpp = a.cp_f[o], rhp = a.rho_f[o];
+        const double por = amean2(phic, php, dd, dp);
+        const double lf = harm2w(lfc, lfp, dd, dp, dd / lfc, dp / lfp);
+        const double lr = harm2w(lrc, lrp, dd, dp, dd / lrc, dp / lrp);
+        const double cpf = harm2w(cpc, cpp, dd, dp, dd / cpc, dp / cpp);
+        rc = harm2w(rhc, rhp, dd, dp, dd / rhc, dp / rhp) * cpf;
+        k1 = (1 - por) * lr + por * lf;
+    }
+    k1_out[c] = k1;
+    rc_out[c] = rc;
+}
+
 // compute_C, one axis (tse.py:811-861): x -> (A, B, N, H, M, G), y -> (C, D,
-// P, J, O, I), z -> (E, F, R, L, Q, K)
-__device__ __forceinline__ AxisTerms species_axis(const double* __restrict__ Df,
-                                                  const double* __restrict__ phi,
+// P, J, O, I), z -> (E, F, R, L, Q, K); Pf: this axis's face values
+__device__ __forceinline__ AxisTerms species_axis(const double* __restrict__ Pf,
                                                   const double* __restrict__ Xn,
                                                   const double* __restrict__ q,
                                                   const double* __restrict__ d, long long c,
                                                   long long st, int ii, bool hp, bool hm,
-                                                  double phic, double DdP, double DdM) {
+                                                  double DdP, double DdM) {
     AxisTerms r = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     const long long op = hp ? c + st : c, om = hm ? c - st : c;
     const double dd = d[ii], dp = d[hp ? ii + 1 : ii], dm = d[hm ? ii - 1 : ii];
-    const double Dc = Df[c], Dp = Df[op], Dm = Df[om];
-    const double pp = phi[op], pm = phi[om];
     const double xp = Xn[op], xm = Xn[om];
     const double qc = q[c], qm = q[om];
-    const double wc = dd / Dc;
+    const double fp = Pf[c], fm = Pf[om];
     const double z = zero_over(dd);
     if (hp) {
         const double dd2 = (0.5 * (dp + dd)) * dd;
-        const double ph = amean2(pp, phic, dp, dd);
-        r.dP = (harm2w(Dp, Dc, dp, dd, dp / Dp, wc) * ph + DdP) / dd2;
+        r.dP = (fp + DdP) / dd2;
         const double qd = qc / dd;
         r.minP = (0.0 < qc) ? z : qd;
         r.maxP = (0.0 > qc) ? z : qd;
@@ -164,8 +202,7 @@ __device__ __forceinline__ AxisTerms species_axis(const double* __restrict__ Df,
     }
     if (hm) {
         const double dd2 = (0.5 * (dm + dd)) * dd;
-        const double ph = amean2(pm, phic, dm, dd);
-        r.dM = (harm2w(Dm, Dc, dm, dd, dm / Dm, wc) * ph + DdM) / dd2;
+        r.dM = (fm + DdM) / dd2;
         const double qd = qm / dd;
         r.maxM = (0.0 > qm) ? z : qd;
         r.minM = (0.0 < qm) ? z : qd;
@@ -175,9 +212,10 @@ __device__ __forceinline__ AxisTerms species_axis(const double* __restrict__ Df,
     return r;
 }
 
-// compute_T, one axis (tse.py:952-1027): the face means of porosity,
-// conductivities, heat capacity and density, then the coefficients
-__device__ __forceinline__ AxisTerms heat_axis(const TseHeatArgs& a, const double* __restrict__ Xn,
+// compute_T, one axis (tse.py:952-1027); K1, RC: this axis's face values
+// (conductivity mix, rho_f cp_f mean)
+__device__ __forceinline__ AxisTerms heat_axis(const double* __restrict__ K1, const double* __restrict__ RC,
+                                               const double* __restrict__ Xn,
                                                const double* __restrict__ q,
                                                const double* __restrict__ d, long long c,
                                                long long st, int ii, bool hp, bool hm,
@@ -185,19 +223,11 @@ __device__ __forceinline__ AxisTerms heat_axis(const TseHeatArgs& a, const doubl
     AxisTerms r = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
     const long long op = hp ? c + st : c, om = hm ? c - st : c;
     const double dd = d[ii], dp = d[hp ? ii + 1 : ii], dm = d[hm ? ii - 1 : ii];
-    const double phic = a.phi[c], lfc = a.l_f[c], lrc = a.l_r[c], cpc = a.cp_f[c], rhc = a.rho_f[c];
-    const double wlf = dd / lfc, wlr = dd / lrc, wcp = dd / cpc, wrh = dd / rhc;
     const double qc = q[c], qm = q[om];
     if (hp) {
         const double dd2 = (0.5 * (dp + dd)) * dd;
-        const double php = a.phi[op], lfp = a.l_f[op], lrp = a.l_r[op], cpp = a.cp_f[op],
-                     rhp = a.rho_f[op];
-        const double por = amean2(phic, php, dd, dp);
-        const double lf = harm2w(lfc, lfp, dd, dp, wlf, dp / lfp);
-        const double lr = harm2w(lrc, lrp, dd, dp, wlr, dp / lrp);
-        const double cpf = harm2w(cpc, cpp, dd, dp, wcp, dp / cpp);
-        const double rhocpf = harm2w(rhc, rhp, dd, dp, wrh, dp / rhp) * cpf;
-        r.dP = ((1 - por) * lr + por * lf + DdP * rhocpf) / dd2;
+        const double rhocpf = RC[c];
+        r.dP = (K1[c] + DdP * rhocpf) / dd2;
         const double S = rhocpf / dd;
         r.minP = min0(qc) * S;
         r.maxP = max0(qc) * S;
@@ -206,14 +236,8 @@ __device__ __forceinline__ AxisTerms heat_axis(const TseHeatArgs& a, const doubl
     }
     if (hm) {
         const double dd2 = (0.5 * (dm + dd)) * dd;
-        const double phm = a.phi[om], lfm = a.l_f[om], lrm = a.l_r[om], cpm = a.cp_f[om],
-                     rhm = a.rho_f[om];
-        const double por = amean2(phic, phm, dd, dm);
-        const double lf = harm2w(lfc, lfm, dd, dm, wlf, dm / lfm);
-        const double lr = harm2w(lrc, lrm, dd, dm, wlr, dm / lrm);
-        const double cpf = harm2w(cpc, cpm, dd, dm, wcp, dm / cpm);
-        const double rhocpf = harm2w(rhc, rhm, dd, dm, wrh, dm / rhm) * cpf;
-        r.dM = ((1 - por) * lr + por * lf + DdM * rhocpf) / dd2;
+        const double rhocpf = RC[om];
+        r.dM = (K1[om] + DdM * rhocpf) / dd2;
         const double S = rhocpf / dd;
         r.maxM = max0(qm) * S;
         r.minM = min0(qm) * S;
@@ -256,19 +280,21 @@ __device__ __forceinline__ void combine_axes(const AxisTerms& X, const AxisTerms
 
 // coefficient part of compute_C.solve (tse.py:795-868)
 __device__ __forceinline__ void species_terms(const TseGrid& g, const TseSpeciesArgs& a,
-                                              const CellIdx& x, const Layout& L, TransportTerms& T) {
+                                              const CellIdx& x, const Layout& L,
+                                              const double* __restrict__ faces, TransportTerms& T) {
     const int nx = L.nx, ny = L.ny, nz = L.nz, i = x.i, j = x.j, k = x.k;
     const long long c = x.c;
     double Dd[6] = {0, 0, 0, 0, 0, 0};
     if (a.l_l[c] != 0 || a.l_t[c] != 0)
         dispersivity_dev(a.qx, a.qy, a.qz, a.l_l, a.l_t, a.BC, i, j, k, nx, ny, nz, Dd);
+    const long long n = (long long)nx * ny * nz;
+    const AxisTerms X = species_axis(faces, a.C, a.qx, g.dx, c, (long long)ny * nz, i, i != nx - 1,
+                                     i != 0, Dd[3], Dd[0]);
+    const AxisTerms Y = species_axis(faces + n, a.C, a.qy, g.dy, c, nz, j, j != ny - 1, j != 0,
+                                     Dd[4], Dd[1]);
+    const AxisTerms Z = species_axis(faces + 2 * n, a.C, a.qz, g.dz, c, 1, k, k != nz - 1, k != 0,
+                                     Dd[5], Dd[2]);
     const double phic = a.phi[c];
-    const AxisTerms X = species_axis(a.D_fx, a.phi, a.C, a.qx, g.dx, c, (long long)ny * nz, i,
-                                     i != nx - 1, i != 0, phic, Dd[3], Dd[0]);
-    const AxisTerms Y = species_axis(a.D_fy, a.phi, a.C, a.qy, g.dy, c, nz, j, j != ny - 1, j != 0,
-                                     phic, Dd[4], Dd[1]);
-    const AxisTerms Z = species_axis(a.D_fz, a.phi, a.C, a.qz, g.dz, c, 1, k, k != nz - 1, k != 0,
-                                     phic, Dd[5], Dd[2]);
     const double Xn = a.C[c];
     combine_axes(X, Y, Z, Xn, T);
     T.Rnum = a.RC[c] * phic;
@@ -280,16 +306,20 @@ __device__ __forceinline__ void species_terms(const TseGrid& g, const TseSpecies
 
 // coefficient part of compute_T.solve (tse.py:930-1036)
 __device__ __forceinline__ void heat_terms(const TseGrid& g, const TseHeatArgs& a, const CellIdx& x,
-                                           const Layout& L, TransportTerms& T) {
+                                           const Layout& L, const double* __restrict__ faces,
+                                           TransportTerms& T) {
     const int nx = L.nx, ny = L.ny, nz = L.nz, i = x.i, j = x.j, k = x.k;
     const long long c = x.c;
     double Dd[6] = {0, 0, 0, 0, 0, 0};
     if (a.l_l[c] != 0 || a.l_t[c] != 0)
         dispersivity_dev(a.qx, a.qy, a.qz, a.l_l, a.l_t, a.BT, i, j, k, nx, ny, nz, Dd);
-    const AxisTerms X = heat_axis(a, a.T, a.qx, g.dx, c, (long long)ny * nz, i, i != nx - 1, i != 0,
-                                  Dd[3], Dd[0]);
-    const AxisTerms Y = heat_axis(a, a.T, a.qy, g.dy, c, nz, j, j != ny - 1, j != 0, Dd[4], Dd[1]);
-    const AxisTerms Z = heat_axis(a, a.T, a.qz, g.dz, c, 1, k, k != nz - 1, k != 0, Dd[5], Dd[2]);
+    const long long n = (long long)nx * ny * nz;
+    const AxisTerms X = heat_axis(faces, faces + 3 * n, a.T, a.qx, g.dx, c, (long long)ny * nz, i,
+                                  i != nx - 1, i != 0, Dd[3], Dd[0]);
+    const AxisTerms Y = heat_axis(faces + n, faces + 4 * n, a.T, a.qy, g.dy, c, nz, j, j != ny - 1,
+                                  j != 0, Dd[4], Dd[1]);
+    const AxisTerms Z = heat_axis(faces + 2 * n, faces + 5 * n, a.T, a.qz, g.dz, c, 1, k, k != nz - 1,
+                                  k != 0, Dd[5], Dd[2]);
     const double Xn = a.T[c];
     combine_axes(X, Y, Z, Xn, T);
     const double por_ = a.phi[c];
@@ -361,15 +391,33 @@ __device__ __forceinline__ void store_dc(const TransportForm& F, const DcFuse& f
 struct SpeciesKind {
     using Args = TseSpeciesArgs;
     static __device__ __forceinline__ void terms(const TseGrid& g, const Args& a, const CellIdx& x,
-                                                 const Layout& L, TransportTerms& T) {
-        species_terms(g, a, x, L, T);
+                                                 const Layout& L, const double* faces,
+                                                 TransportTerms& T) {
+        species_terms(g, a, x, L, faces, T);
+    }
+    // the face pass, one cell (natural order)
+    static __device__ __forceinline__ void faces(const TseGrid& g, const Args& a, const Layout& L,
+                                                 long long c, int i, int j, int k, double* out) {
+        const long long n = (long long)L.nx * L.ny * L.nz;
+        const double phic = a.phi[c];
+        species_face(a.D_fx, a.phi, g.dx, c, (long long)L.ny * L.nz, i, i != L.nx - 1, phic, out);
+        species_face(a.D_fy, a.phi, g.dy, c, L.nz, j, j != L.ny - 1, phic, out + n);
+        species_face(a.D_fz, a.phi, g.dz, c, 1, k, k != L.nz - 1, phic, out + 2 * n);
     }
 };
 struct HeatKind {
     using Args = TseHeatArgs;
     static __device__ __forceinline__ void terms(const TseGrid& g, const Args& a, const CellIdx& x,
-                                                 const Layout& L, TransportTerms& T) {
-        heat_terms(g, a, x, L, T);
+                                                 const Layout& L, const double* faces,
+                                                 TransportTerms& T) {
+        heat_terms(g, a, x, L, faces, T);
+    }
+    static __device__ __forceinline__ void faces(const TseGrid& g, const Args& a, const Layout& L,
+                                                 long long c, int i, int j, int k, double* out) {
+        const long long n = (long long)L.nx * L.ny * L.nz;
+        heat_face(a, g.dx, c, (long long)L.ny * L.nz, i, i != L.nx - 1, out, out + 3 * n);
+        heat_face(a, g.dy, c, L.nz, j, j != L.ny - 1, out + n, out + 4 * n);
+        heat_face(a, g.dz, c, 1, k, k != L.nz - 1, out + 2 * n, out + 5 * n);
     }
 };
 
@@ -388,7 +436,8 @@ constexpr int kAssembleMinBlocks = TSE_ASM_MINB;
 template <class Kind, bool DC>
 __device__ __forceinline__ void assemble_body(const TseGrid& g, const typename Kind::Args& a,
                                               const TransportForm& F, uint8_t* mask0,
-                                              uint8_t* mask1, const Layout& L, const DcFuse& fz) {
+                                              uint8_t* mask1, const Layout& L,
+                                              const double* __restrict__ faces, const DcFuse& fz) {
     __shared__ double sh[kBlock / 32];
     double x2 = 0.0;
     const int per = DC ? fz.per_thread : 1;
@@ -403,7 +452,7 @@ __device__ __forceinline__ void assemble_body(const TseGrid& g, const typename K
             continue;
         }
         TransportTerms T;
-        Kind::terms(g, a, x, L, T);
+        Kind::terms(g, a, x, L, faces, T);
         store_terms(F, msk, x, T, L.nx, L.ny, L.nz);
         if (DC) {
             store_dc(F, fz, x, &T);
@@ -420,16 +469,27 @@ __device__ __forceinline__ void assemble_body(const TseGrid& g, const typename K
 template <bool DC>
 __global__ void __launch_bounds__(kBlock, kAssembleMinBlocks)
     assemble_c_kernel(TseGrid g, TseSpeciesArgs a, TransportForm F, uint8_t* mask0, uint8_t* mask1,
-                      Layout L, DcFuse fz) {
-    assemble_body<SpeciesKind, DC>(g, a, F, mask0, mask1, L, fz);
+                      Layout L, const double* faces, DcFuse fz) {
+    assemble_body<SpeciesKind, DC>(g, a, F, mask0, mask1, L, faces, fz);
 }
 
 // coefficient part of compute_T.solve (tse.py:930-1036)
 template <bool DC>
 __global__ void __launch_bounds__(kBlock, kAssembleMinBlocks)
     assemble_t_kernel(TseGrid g, TseHeatArgs a, TransportForm F, uint8_t* mask0, uint8_t* mask1,
-                      Layout L, DcFuse fz) {
-    assemble_body<HeatKind, DC>(g, a, F, mask0, mask1, L, fz);
+                      Layout L, const double* faces, DcFuse fz) {
+    assemble_body<HeatKind, DC>(g, a, F, mask0, mask1, L, faces, fz);
+}
+
+// the face pass before an assembly: one thread per cell, natural order
+template <class Kind>
+__global__ void faces_kernel(TseGrid g, typename Kind::Args a, Layout L, double* faces) {
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= (long long)L.nx * L.ny * L.nz) return;
+    int i, j, k;
+    long long row;
+    grid_coords(c, L.ny, L.nz, i, j, k, row);
+    Kind::faces(g, a, L, c, i, j, k, faces);
 }
 
 __global__ void unpack_t_kernel(double* out, const double* X0, const double* X1, Layout L) {
@@ -443,6 +503,9 @@ __global__ void unpack_t_kernel(double* out, const double* X0, const double* X1,
     out[t] = ((i + j + k) & 1) ? X1[m] : X0[m];
 }
 
+// face values a cell: 3 for a species, 6 for heat
+constexpr int kTransportFaceWords = 6;
+
 size_t transport_ws_bytes(const Layout& L, long long* Ncal_out) {
     long long Ncal = (L.Nc + 31) & ~31LL;
     if (Ncal_out) *Ncal_out = Ncal;
@@ -451,11 +514,10 @@ size_t transport_ws_bytes(const Layout& L, long long* Ncal_out) {
     b += align256((size_t)2 * kMaxBlocks * sizeof(double));
     b += 2 * align256((size_t)Ncal);
     b += 2 * (size_t)TA_COUNT * Ncal * sizeof(double);
+    b += align256((size_t)kTransportFaceWords * L.nx * L.ny * L.nz * sizeof(double));   // face pass
     return b;
 }
 
-// Carve the workspace and launch the assembly (shared by the exact and the
-// defect-correction transport solves).
 // Carve the workspace (shared by the exact and the defect-correction
 // transport solves) and reset the grid barrier.
 template <class Args>
@@ -475,6 +537,7 @@ static int carve_transport(const TseGrid* grid, const Args* a, void* d_ws, size_
     p += align256((size_t)S.Ncal);
     S.F.arr[0] = (double*)p;
     S.F.arr[1] = S.F.arr[0] + (size_t)TA_COUNT * S.Ncal;
+    S.faces = S.F.arr[1] + (size_t)TA_COUNT * S.Ncal;
     S.F.Ncal = S.Ncal;
     S.F.SX = S.L.SX;
     S.F.H = S.L.H;
@@ -489,26 +552,38 @@ static int carve_transport(const TseGrid* grid, const Args* a, void* d_ws, size_
 }
 
 // carve + the exact form's assembly
-template <class Args, class AssembleK>
+// the face pass of a transport setup
+template <class Args, class FacesK>
+static void launch_faces(const TseGrid* grid, const Args* a, const TransportSetup& S, FacesK fk,
+                         cudaStream_t stream) {
+    const long long n = (long long)S.L.nx * S.L.ny * S.L.nz;
+    fk<<<(unsigned)((n + kBlock - 1) / kBlock), kBlock, 0, stream>>>(*grid, *a, S.L, S.faces);
+}
+
+// carve + the face pass + the exact form's assembly
+template <class Args, class FacesK, class AssembleK>
 static int setup_transport(const TseGrid* grid, const Args* a, void* d_ws, size_t ws_bytes,
-                           cudaStream_t stream, AssembleK kernel, int imbl, TransportSetup& S) {
+                           cudaStream_t stream, FacesK fk, AssembleK kernel, int imbl,
+                           TransportSetup& S) {
     int rc = carve_transport(grid, a, d_ws, ws_bytes, stream, imbl, S);
     if (rc != TSE_OK) return rc;
+    launch_faces(grid, a, S, fk, stream);
     const long long total = (long long)S.L.nx * S.L.ny * S.L.nzp;
     kernel<<<(unsigned)((total + kBlock - 1) / kBlock), kBlock, 0, stream>>>(
-        *grid, *a, S.F, S.mask[0], S.mask[1], S.L, DcFuse{});
+        *grid, *a, S.F, S.mask[0], S.mask[1], S.L, S.faces, DcFuse{});
     return cudaGetLastError() == cudaSuccess ? TSE_OK : TSE_ERR_LAUNCH;
 }
 
 // carve + the assembly that also writes the mixed-precision form's first
 // cycle (records, r', x^2 partials); *nparts: the number of partials
-template <class Args, class AssembleK>
+template <class Args, class FacesK, class AssembleK>
 static int setup_transport_dc(const TseGrid* grid, const Args* a, void* d_ws, size_t ws_bytes,
-                              cudaStream_t stream, AssembleK kernel, int imbl, TransportSetup& S,
-                              int* nparts) {
+                              cudaStream_t stream, FacesK fk, AssembleK kernel, int imbl,
+                              TransportSetup& S, int* nparts) {
     int rc = carve_transport(grid, a, d_ws, ws_bytes, stream, imbl, S);
     if (rc != TSE_OK) return rc;
     if (S.tail_bytes < dc_extra_bytes(S.L)) return TSE_ERR_WORKSPACE;
+    launch_faces(grid, a, S, fk, stream);
     DcCtl c;
     dc_carve(S, c, TA_X);
     long long per, nb;
@@ -519,39 +594,43 @@ static int setup_transport_dc(const TseGrid* grid, const Args* a, void* d_ws, si
     fz.Ncal = c.Ncal;
     fz.partials = S.partials;
     fz.per_thread = (int)per;
-    kernel<<<(unsigned)nb, kBlock, 0, stream>>>(*grid, *a, S.F, S.mask[0], S.mask[1], S.L, fz);
+    kernel<<<(unsigned)nb, kBlock, 0, stream>>>(*grid, *a, S.F, S.mask[0], S.mask[1], S.L, S.faces,
+                                                 fz);
     *nparts = (int)nb;
     return cudaGetLastError() == cudaSuccess ? TSE_OK : TSE_ERR_LAUNCH;
 }
 
 int setup_species(const TseGrid* grid, const TseSpeciesArgs* a, void* d_ws, size_t ws_bytes,
                   cudaStream_t stream, TransportSetup& S) {
-    return setup_transport(grid, a, d_ws, ws_bytes, stream, assemble_c_kernel<false>, a->imblflo, S);
+    return setup_transport(grid, a, d_ws, ws_bytes, stream, faces_kernel<SpeciesKind>,
+                           assemble_c_kernel<false>, a->imblflo, S);
 }
 
 int setup_heat(const TseGrid* grid, const TseHeatArgs* a, void* d_ws, size_t ws_bytes,
                cudaStream_t stream, TransportSetup& S) {
-    return setup_transport(grid, a, d_ws, ws_bytes, stream, assemble_t_kernel<false>, a->imblflo, S);
+    return setup_transport(grid, a, d_ws, ws_bytes, stream, faces_kernel<HeatKind>,
+                           assemble_t_kernel<false>, a->imblflo, S);
 }
 
 int setup_species_dc(const TseGrid* grid, const TseSpeciesArgs* a, void* d_ws, size_t ws_bytes,
                      cudaStream_t stream, TransportSetup& S, int* nparts) {
-    return setup_transport_dc(grid, a, d_ws, ws_bytes, stream, assemble_c_kernel<true>, a->imblflo,
-                              S, nparts);
+    return setup_transport_dc(grid, a, d_ws, ws_bytes, stream, faces_kernel<SpeciesKind>,
+                              assemble_c_kernel<true>, a->imblflo, S, nparts);
 }
 
 int setup_heat_dc(const TseGrid* grid, const TseHeatArgs* a, void* d_ws, size_t ws_bytes,
                   cudaStream_t stream, TransportSetup& S, int* nparts) {
-    return setup_transport_dc(grid, a, d_ws, ws_bytes, stream, assemble_t_kernel<true>, a->imblflo,
-                              S, nparts);
+    return setup_transport_dc(grid, a, d_ws, ws_bytes, stream, faces_kernel<HeatKind>,
+                              assemble_t_kernel<true>, a->imblflo, S, nparts);
 }
 
-template <class Args, class AssembleK>
+template <class Args, class FacesK, class AssembleK>
 static int run_transport(const TseGrid* grid, const Args* a, double* X, TseSolveStatus* d_status,
-                         void* d_ws, size_t ws_bytes, void* stream_, AssembleK kernel, int imbl) {
+                         void* d_ws, size_t ws_bytes, void* stream_, FacesK fk, AssembleK kernel,
+                         int imbl) {
     cudaStream_t stream = (cudaStream_t)stream_;
     TransportSetup S;
-    int rc = setup_transport(grid, a, d_ws, ws_bytes, stream, kernel, imbl, S);
+    int rc = setup_transport(grid, a, d_ws, ws_bytes, stream, fk, kernel, imbl, S);
     if (rc != TSE_OK) return rc;
     const Layout L = S.L;
     TransportForm F = S.F;
@@ -643,7 +722,7 @@ extern "C" int32_t tse_compute_C(const TseGrid* grid, const TseSpeciesArgs* a,
     if (!a->C || !a->D_fx || !a->D_fy || !a->D_fz || !a->phi || !a->rho_f || !a->qx || !a->qy ||
         !a->qz || !a->BC || !a->WC || !a->RC || !a->e || !a->l_l || !a->l_t)
         return TSE_ERR_ARG;
-    return run_transport(grid, a, a->C, d_status, d_ws, ws_bytes, stream,
+    return run_transport(grid, a, a->C, d_status, d_ws, ws_bytes, stream, faces_kernel<SpeciesKind>,
                          assemble_c_kernel<false>, a->imblflo);
 }
 
@@ -655,7 +734,7 @@ extern "C" int32_t tse_compute_T(const TseGrid* grid, const TseHeatArgs* a,
     if (!a->T || !a->l_f || !a->cp_f || !a->rho_f || !a->phi || !a->qx || !a->qy || !a->qz ||
         !a->BT || !a->WT || !a->e || !a->l_r || !a->rho_r || !a->cp_r || !a->l_l || !a->l_t)
         return TSE_ERR_ARG;
-    return run_transport(grid, a, a->T, d_status, d_ws, ws_bytes, stream,
+    return run_transport(grid, a, a->T, d_status, d_ws, ws_bytes, stream, faces_kernel<HeatKind>,
                          assemble_t_kernel<false>, a->imblflo);
 }
 
