@@ -112,12 +112,14 @@ __device__ __forceinline__ bool decode_padded(long long t, const Layout& L, Cell
 }
 
 // The assemblies below keep the reference's operations and their order for
-// every value they produce, and drop only divisions whose quotient is
-// already known:
-//  - harm2(H1, H2, d1, d2) = (d1 + d2) / (d1 / H1 + d2 / H2): a cell's own
-//    quotient d / H is the same in both faces of an axis, so it is formed once;
+// every value they produce, and drop only work whose result is already
+// known:
+//  - each face's means are formed once, by the face pass, rather than by
+//    both cells that share the face (see species_face);
 //  - min0(q) / d and max0(q) / d: one of the two is 0 / d, so q / d is formed
 //    once and 0 / d (+0 for d > 0) is selected for the other.
+// harm2w is harm2(H1, H2, d1, d2) = (d1 + d2) / (d1 / H1 + d2 / H2) with the
+// quotients w1 = d1 / H1, w2 = d2 / H2 passed in.
 __device__ __forceinline__ double harm2w(double H1, double H2, double d1, double d2, double w1,
                                          double w2) {
     if (H1 != 0.0 && H2 != 0.0) return (d1 + d2) / (w1 + w2);
