@@ -423,13 +423,14 @@ struct HeatKind {
     }
 };
 
-// Both assemblies are latency-bound (FP64 divisions and neighbour loads per
-// cell).  Three 256-thread blocks per SM (80 registers, some spilled) rather
-// than the two that ~96 registers allow: measured on the 256 x 256 x 128
-// reservoir, a species solve of 5 iterations took 1.75 ms at three blocks,
-// 2.03 ms at two and 1.74 ms at four (heat, 3 iterations: 1.61, 1.90, 1.63).
+// Both assemblies are bound by the latency of their loads (15 input arrays,
+// neighbours included).  Four 256-thread blocks per SM (64 registers, some
+// spilled): with the face values read from the face pass, measured on the
+// 256 x 256 x 128 reservoir (whole calls, one box, one call each), a species
+// solve of 5 iterations took 1.65 ms at four blocks, 1.89 at three and 2.09 at
+// two (heat, 3 iterations: 1.39, 1.51, 1.65 ms).
 #ifndef TSE_ASM_MINB
-#define TSE_ASM_MINB 3
+#define TSE_ASM_MINB 4
 #endif
 constexpr int kAssembleMinBlocks = TSE_ASM_MINB;
 
