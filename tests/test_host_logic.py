@@ -598,3 +598,35 @@ def test_server_admission_without_and_with_a_slot_limit(monkeypatch):
         assert st["cell_updates"] == 16
         assert state["peak"] == peak, (slots, state["peak"])
         assert len(srv.workers) == workers, (slots, len(srv.workers))
+
+
+def test_face_means_are_the_same_from_either_cell():
+    """The transport assemblies form each face's means once (the face pass)
+    and both cells of the face read them.  That keeps every coefficient bit for
+    bit only because the two cells' expressions differ by commuted operands:
+    harm2(H1, H2, d1, d2) = (d1 + d2) / (d1/H1 + d2/H2) and
+    amean2(X1, X2, d1, d2) = (X1 d1 + X2 d2) / (d1 + d2) with the two cells
+    swapped.  IEEE-754 addition and multiplication commute, which this checks
+    on random float64 operands over many magnitudes (numpy's float64
+    operations round like the GPU's FP64 without contraction)."""
+    import numpy
+    rng = numpy.random.default_rng(7)
+    n = 200000
+    H1, H2 = [10.0 ** rng.uniform(-15, 5, n) for _ in range(2)]
+    X1, X2 = [rng.uniform(-1e3, 1e3, n) for _ in range(2)]
+    d1, d2 = [10.0 ** rng.uniform(-3, 3, n) for _ in range(2)]
+
+    def harm2(a, b, da, db):
+        return (da + db) / (da / a + db / b)
+
+    def amean2(a, b, da, db):
+        return (a * da + b * db) / (da + db)
+
+    assert numpy.array_equal(harm2(H1, H2, d1, d2), harm2(H2, H1, d2, d1))
+    assert numpy.array_equal(amean2(X1, X2, d1, d2), amean2(X2, X1, d2, d1))
+    # the heat face's conductivity mix and the species face's product
+    por = amean2(X1, X2, d1, d2) * 1e-4
+    lr, lf = harm2(H1, H2, d1, d2), harm2(H2 * 3, H1 * 7, d1, d2)
+    lr_s, lf_s = harm2(H2, H1, d2, d1), harm2(H1 * 7, H2 * 3, d2, d1)
+    por_s = amean2(X2, X1, d2, d1) * 1e-4
+    assert numpy.array_equal((1 - por) * lr + por * lf, (1 - por_s) * lr_s + por_s * lf_s)
